@@ -1,0 +1,165 @@
+/*
+ * wmles_cuda.h - C ABI of libwmles_cuda.so, the B200 (sm_100a) implementation of the
+ * wmles explicit RHS + SSP-RK3 step.
+ *
+ * Plain C: raw pointers and sizes, no torch or CUDA types in the signatures (a stream is
+ * passed as `void*` holding a cudaStream_t; NULL = legacy default stream).  Every entry
+ * point returns 0 on success or a negative WM_E* status; wm_last_error() gives the text
+ * of the calling thread's last error.  No C++ exception crosses this boundary.
+ *
+ * Ownership: a wm_case owns its device copies of the metrics, ghost programs, wall
+ * geometry, work buffers (two RK stage states) and reduction scratch; it is created once
+ * per Solver and freed by wm_case_destroy.  State arrays passed to the entry points are
+ * borrowed device pointers (one per block, float64, layout (5, Ni, Nj, Nk) C-order with
+ * Ni = ni + 2 ng ...), used only during the call on the given stream and never freed.
+ *
+ * Reference interfaces replaced (EduardoMolina/wmles_jax):
+ *   wm_case_create   Solver.__init__            wmles/solver.py:40-51 (+ Mesh.finalize output)
+ *   wm_apply_bcs     Solver.apply_bcs           wmles/solver.py:59-73
+ *   wm_rhs           Solver.rhs / _rhs           wmles/solver.py:97-106,159-160
+ *   wm_max_dt        Solver.max_dt / _dt         wmles/solver.py:135-154
+ *   wm_advance       Solver.advance             wmles/solver.py:110-133,156-157
+ *   wm_step          max_dt + advance, as the drivers call them (examples/channel_wmles.py:124-125)
+ *   wm_wall_stats    Solver.wall_stats          wmles/solver.py:163-179
+ */
+#ifndef WMLES_CUDA_H
+#define WMLES_CUDA_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WM_ABI_VERSION 1
+#define WM_MAX_BLOCKS 96      /* blocks per case (all cases of one batched launch) */
+#define WM_NMET 14            /* metric components per cell, see WM_MET_* */
+
+/* status codes */
+#define WM_OK 0
+#define WM_E_INVALID (-1)     /* malformed descriptor or argument */
+#define WM_E_CUDA (-2)        /* a CUDA runtime call failed */
+#define WM_E_NONFINITE (-3)   /* non-finite or non-positive dt / state detected */
+#define WM_E_UNSUPPORTED (-4) /* option not built into this library */
+
+/* metric component order (per cell, float64): face area vector of the cell's LOWER face
+ * in each direction (the reference's S[d][:, c] for face index c), volume, centre, and
+ * the SGS filter width V^(1/3) */
+enum { WM_MET_SIX = 0, WM_MET_SIY, WM_MET_SIZ, WM_MET_SJX, WM_MET_SJY, WM_MET_SJZ,
+       WM_MET_SKX, WM_MET_SKY, WM_MET_SKZ, WM_MET_VOL, WM_MET_XCX, WM_MET_XCY, WM_MET_XCZ,
+       WM_MET_DELTA };
+
+enum { WM_SCHEME_KEP = 0, WM_SCHEME_MUSCL = 1, WM_SCHEME_HYBRID = 2 };
+enum { WM_LIMITER_ALBADA = 0, WM_LIMITER_MINMOD = 1 };
+enum { WM_SGS_NONE = 0, WM_SGS_SMAGORINSKY = 1, WM_SGS_WALE = 2, WM_SGS_VREMAN = 3 };
+enum { WM_PREC_FP64 = 0, WM_PREC_MIXED = 1 };
+
+/* ghost-cell program: every listed ghost cell is a chain of per-cell maps applied to
+ * one source value (an interior cell, an inflow value or a constant) */
+enum { WM_SRC_CELL = 0, WM_SRC_INFLOW = 1, WM_SRC_CONST = 2 };
+enum { WM_OP_SLIP = 1, WM_OP_NOSLIP = 2, WM_OP_FARFIELD = 3 };
+
+typedef struct {
+    double gamma, R, Pr, Pr_t, mu_ref, T_ref, S_suth;
+} wm_gas;
+
+typedef struct {
+    int n[3];                 /* interior cells per direction */
+    int ng;                   /* ghost layers (the reference's ng = 3) */
+    const double* metrics;    /* host, WM_NMET x Ni x Nj x Nk */
+} wm_block;
+
+typedef struct {
+    int block, axis, side;    /* the wall-modelled face */
+    int n_match;              /* sample cell counted from the wall (1 = first cell) */
+    int isothermal;           /* 0: adiabatic (recovery temperature, q_w = 0) */
+    double T_wall;
+    double kappa, B;
+    int n_iter;               /* Newton iterations on Spalding's law */
+    const double* geom;       /* host, 5 x nt1 x nt2: |S|, n_out (3), h; tangential axes
+                                 in increasing order, interior extent */
+} wm_wall;
+
+typedef struct {
+    int count;                /* ghost cells to write */
+    const int* dst;           /* 2*count: block, flat cell index */
+    const int* src;           /* 2*count: (kind << 24) | block (or BC id for CONST), flat index */
+    const int* ops;           /* 2*count: first op, number of ops (applied in order) */
+    int nops;
+    const int* op_code;       /* nops: code | (bc id << 8) | (side << 16) */
+    const double* op_nrm;     /* 3*nops: unit normal of the boundary face */
+} wm_ghost_program;
+
+typedef struct {
+    int block;                /* i-min face of this block */
+    int n_modes, n_tab;
+    const double* modes;      /* host, 3 x 4 x n_modes: kx, ky, kz, phase per component */
+    const double* table;      /* host, n_tab x 7: y/L, U, V, uu, vv, ww, uv (by U_inf) */
+    double U_inf, L, rho_inf, p_inf;
+} wm_inflow;
+
+typedef struct {
+    int enabled;
+    double x_start_l, x_end_l, strength, U_inf, L;
+} wm_sponge;
+
+typedef struct {
+    wm_gas gas;
+    int scheme;               /* WM_SCHEME_* */
+    int kep_order;            /* 2 or 4 (central flux of KEP and of Hybrid) */
+    int limiter;              /* WM_LIMITER_* (MUSCL and Hybrid) */
+    double th0, th1;          /* Hybrid switch thresholds */
+    int sgs;                  /* WM_SGS_* */
+    double sgs_coeff;         /* Cs, Cw or Cs (Vreman) */
+    double cfl;
+    int precision;            /* WM_PREC_* */
+    int cmf_dir;              /* ConstantMassFlux direction, -1 = none */
+    double cmf_target;
+    double cmf_volume;        /* sum of interior volumes, as the reference sums them */
+    int nblocks;
+    const wm_block* blocks;
+    int nwalls;
+    const wm_wall* walls;
+    int nbc;
+    const double* bc_table;   /* 8 per BC: const state / prim_inf (5), T_wall, isothermal, 0 */
+    wm_ghost_program ghost_rhs;   /* ghost cells read by the RHS */
+    wm_ghost_program ghost_all;   /* every ghost cell (apply_bcs) */
+    const wm_inflow* inflow;      /* NULL if no synthetic-turbulence inflow */
+    wm_sponge sponge;
+    int tile;                 /* stage-kernel tile shape id, -1 = automatic */
+    int chunk;                /* planes per CTA along i, 0 = automatic */
+} wm_case_desc;
+
+typedef struct wm_case wm_case;
+
+int wm_version(void);
+const char* wm_last_error(void);
+
+int wm_case_create(const wm_case_desc* desc, wm_case** out);
+void wm_case_destroy(wm_case* c);
+
+/* Fill every ghost cell of q (in place) at `time`. */
+int wm_apply_bcs(wm_case* c, double* const* q, double time, void* stream);
+
+/* r = RHS(q) on the interior (ghost cells of r are left untouched); fills the ghost
+ * cells of q it reads, in place. */
+int wm_rhs(wm_case* c, double* const* q, double* const* r, double time, void* stream);
+
+/* CFL time step of q, written to dt_dev (device double).  Interior only; q is not
+ * modified. */
+int wm_max_dt(wm_case* c, const double* const* q, double* dt_dev, void* stream);
+
+/* One SSP-RK3 step (plus the case's constraint) of q_in with the device time step
+ * *dt_dev, written to q_out (interior).  Ghost cells of q_in are refreshed in place. */
+int wm_advance(wm_case* c, double* const* q_in, double* const* q_out, const double* dt_dev,
+               double time, void* stream);
+
+/* dt = max_dt(q_in) written to dt_dev, then advance(q_in -> q_out, dt). */
+int wm_step(wm_case* c, double* const* q_in, double* const* q_out, double* dt_dev,
+            double time, void* stream);
+
+/* (tau_w, q_w) of every wall-modelled face: out[w] is a device buffer of 2 x nt1 x nt2. */
+int wm_wall_stats(wm_case* c, const double* const* q, double* const* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WMLES_CUDA_H */

@@ -1,0 +1,341 @@
+// Surface and reduction kernels of the step: wall-model flux override, CFL time step with
+// the constant-mass-flux update, sponge spanwise means and synthetic-turbulence inflow.
+#include <cfloat>
+#include "physics.cuh"
+#include "aux.cuh"
+
+namespace wm {
+
+__device__ __forceinline__ long long cell_index(const BlockDev& B, int axis, int c, int a, int b) {
+    // cell at position c along `axis`, (a, b) on the other two axes in increasing order
+    const int Nj = B.N[1], Nk = B.N[2];
+    if (axis == 0) return ((long long)c * Nj + a) * Nk + b;
+    if (axis == 1) return ((long long)a * Nj + c) * Nk + b;
+    return ((long long)a * Nj + b) * Nk + c;
+}
+
+__device__ __forceinline__ double sutherland_d(double T, const CaseDev& C) {
+    return C.mu_ref * pow(T * C.inv_Tref, 1.5) * C.TrefS / (T + C.S_suth);
+}
+
+// ------------------------------------------------------------------ wall model
+// WallModel.wall_flux (wmles/bc.py:145-166) with EquilibriumWallModel (wmles/wall_model.py:42-61)
+__global__ void wall_kernel(const __grid_constant__ WallArgs A) {
+    const WallDev& W = A.walls[blockIdx.y];
+    const long long nf = (long long)W.nt1 * W.nt2;
+    const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nf) return;
+    const BlockDev& B = A.blocks[W.block];
+    const CaseDev& C = A.cases[B.case_id];
+    const int ng = B.ng, n = B.n[W.axis];
+    const int a = int(f / W.nt2) + ng, b = int(f % W.nt2) + ng;
+    const int mi = W.side == 0 ? ng + W.n_match - 1 : ng + n - W.n_match;
+    const int ci = W.side == 0 ? ng : ng + n - 1;
+    const double* q = A.q[W.block];
+    const long long N = B.ncell;
+    const long long im = cell_index(B, W.axis, mi, a, b), ic = cell_index(B, W.axis, ci, a, b);
+    const double rho = q[im];
+    const double u[3] = {q[N + im] / rho, q[2 * N + im] / rho, q[3 * N + im] / rho};
+    const double ke = (u[0] * u[0] + u[1] * u[1]) + u[2] * u[2];
+    const double p_h = C.gm1 * (q[4 * N + im] - 0.5 * rho * ke);
+    const double T_h = p_h / (rho * C.Rg);
+    const double rb = q[ic];
+    const double ub[3] = {q[N + ic] / rb, q[2 * N + ic] / rb, q[3 * N + ic] / rb};
+    const double p_b = C.gm1 * (q[4 * N + ic] - 0.5 * rb * ((ub[0] * ub[0] + ub[1] * ub[1]) + ub[2] * ub[2]));
+    const double Sm = W.geom[f], nrm[3] = {W.geom[nf + f], W.geom[2 * nf + f], W.geom[3 * nf + f]};
+    const double h = W.geom[4 * nf + f];
+    const double un = (u[0] * nrm[0] + u[1] * nrm[1]) + u[2] * nrm[2];
+    const double up[3] = {u[0] - un * nrm[0], u[1] - un * nrm[1], u[2] - un * nrm[2]};
+    const double U = sqrt((up[0] * up[0] + up[1] * up[1]) + up[2] * up[2] + 1e-20);
+    // equilibrium model
+    const double Um = fmax(U, 1e-8);
+    const double T_w = W.isothermal ? W.T_wall : T_h + A.Pr13 * (Um * Um) / (2.0 * C.cp);
+    const double rho_w = p_h / (C.Rg * T_w);
+    const double mu_w = sutherland_d(T_w, C);
+    const double ut = spalding_utau(W.kappa, W.ekb, W.n_iter, h, Um, rho_w, mu_w);
+    const double tau = rho_w * (ut * ut);
+    double qw = 0.0;
+    if (W.isothermal) {
+        // Kader (1981) temperature law
+        const double Pr = C.Pr;
+        const double yp = fmax(h * ut * rho_w / mu_w, 1e-6);
+        const double x = Pr * yp, x2 = x * x;
+        const double Gam = fmax(0.01 * (x2 * x2) / (1.0 + 5.0 * A.Pr3 * yp), 1e-20);
+        const double Tp = Pr * yp * exp(-Gam) + (2.12 * log(1.0 + yp) + A.kader_beta) * exp(-1.0 / Gam);
+        qw = rho_w * C.cp * ut * (T_w - T_h) / Tp;
+    }
+    const double sgn = W.side == 1 ? 1.0 : -1.0;
+    W.F[f] = 0.0;
+#pragma unroll
+    for (int v = 0; v < 3; ++v) W.F[(1 + v) * nf + f] = sgn * ((p_b * nrm[v] + tau * (up[v] / U)) * Sm);
+    W.F[4 * nf + f] = sgn * (-qw * Sm);
+    W.tq[f] = tau;
+    W.tq[nf + f] = qw;
+}
+
+cudaError_t launch_wall(const WallArgs& W, cudaStream_t s) {
+    if (W.nwalls == 0) return cudaSuccess;
+    dim3 grid((W.max_faces + 127) / 128, W.nwalls);
+    wall_kernel<<<grid, 128, 0, s>>>(W);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ reductions
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < NT / 32; ++w) s += red[w];
+    __syncthreads();
+    if (threadIdx.x == 0) red[0] = s;
+    __syncthreads();
+    const double r = red[0];
+    __syncthreads();
+    return r;
+}
+
+template <int NT>
+__device__ __forceinline__ double block_min(double v, double* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_down_sync(0xffffffffu, v, o));
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double m = DBL_MAX;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < NT / 32; ++w) m = fmin(m, red[w]);
+    return m;   // valid in thread 0
+}
+
+// CFL time step (Solver._dt, wmles/solver.py:135-151), optionally after applying the
+// constant-mass-flux shift (ConstantMassFlux.__call__, wmles/solver.py:22-36) in place.
+constexpr int DT_NT = 256;
+__global__ void __launch_bounds__(DT_NT) dt_kernel(const __grid_constant__ DtArgs D) {
+    __shared__ double red[DT_NT / 32];
+    __shared__ bool last;
+    const int b = blockIdx.y;
+    const BlockDev& B = D.blocks[b];
+    const CaseDev& C = D.cases[B.case_id];
+    const bool cmf = D.cmf_part != nullptr && C.cmf_dir >= 0;
+    double delta = 0.0;
+    if (cmf) {
+        double s = 0.0;
+        for (int i = threadIdx.x; i < D.cmf_nparts; i += DT_NT) s += D.cmf_part[i];
+        s = block_sum<DT_NT>(s, red);
+        delta = C.cmf_target - s / C.cmf_volume;
+    }
+    const int ng = B.ng, ni = B.n[0], nj = B.n[1], nk = B.n[2];
+    const int Nj = B.N[1], Nk = B.N[2];
+    const long long N = B.ncell, plane = B.plane;
+    const long long ncells = (long long)ni * nj * nk;
+    double* q = D.q[b];
+    const double* met = B.met;
+    double dtmin = DBL_MAX;
+    for (long long c = (long long)blockIdx.x * DT_NT + threadIdx.x; c < ncells; c += (long long)gridDim.x * DT_NT) {
+        const int i = int(c / ((long long)nj * nk)) + ng;
+        const int r = int(c % ((long long)nj * nk));
+        const int j = r / nk + ng, k = r % nk + ng;
+        const long long idx = i * plane + (long long)j * Nk + k;
+        double qv[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) qv[v] = q[v * N + idx];
+        if (cmf) {
+            const int m = 1 + C.cmf_dir;
+            const double dE = (2.0 * qv[m] * delta + delta * delta) / (2.0 * qv[0]);
+            qv[m] = qv[m] + delta;
+            qv[4] = qv[4] + dE;
+            q[m * N + idx] = qv[m];
+            q[4 * N + idx] = qv[4];
+        }
+        if (!D.want_dt) continue;
+        const double rho = qv[0];
+        const double u = qv[1] / rho, v = qv[2] / rho, w = qv[3] / rho;
+        const double p = C.gm1 * (qv[4] - 0.5 * rho * ((u * u + v * v) + w * w));
+        const double T = p / (rho * C.Rg);
+        const double cs = sqrt(C.gamma * C.Rg * T);
+        const double nu = C.nu_fac * sutherland_d(T, C) / rho;
+        const double vol = met[WM_MET_VOL * N + idx];
+        double lam = 0.0, lamv = 0.0;
+        const long long off[3] = {plane, Nk, 1};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double* S = met + (3 * d) * N;
+            const double sx = 0.5 * (S[idx] + S[idx + off[d]]);
+            const double sy = 0.5 * (S[N + idx] + S[N + idx + off[d]]);
+            const double sz = 0.5 * (S[2 * N + idx] + S[2 * N + idx + off[d]]);
+            const double Sm = sqrt((sx * sx + sy * sy) + sz * sz);
+            lam = lam + fabs((u * sx + v * sy) + w * sz) + cs * Sm;
+            lamv = lamv + nu * (Sm * Sm) / vol;
+        }
+        dtmin = fmin(dtmin, C.cfl / ((lam + 4.0 * lamv) / vol));
+    }
+    if (!D.want_dt) return;
+    const double m = block_min<DT_NT>(dtmin, red);
+    const int nparts = D.nblocks * D.ctas_per_block;
+    if (threadIdx.x == 0) {
+        D.dt_part[b * D.ctas_per_block + blockIdx.x] = m;
+        __threadfence();
+        const unsigned prev = atomicAdd(D.counter, 1u);
+        last = (prev == unsigned(nparts - 1));
+    }
+    __syncthreads();
+    if (last) {
+        __threadfence();
+        double mm = DBL_MAX;
+        for (int i = threadIdx.x; i < nparts; i += DT_NT) mm = fmin(mm, ((volatile double*)D.dt_part)[i]);
+        mm = block_min<DT_NT>(mm, red);
+        if (threadIdx.x == 0) {
+            D.dt_out[0] = mm;
+            *D.counter = 0u;
+        }
+    }
+}
+
+cudaError_t launch_dt(const DtArgs& D, cudaStream_t s) {
+    dim3 grid(D.ctas_per_block, D.nblocks);
+    dt_kernel<<<grid, DT_NT, 0, s>>>(D);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ sponge
+// volume-weighted spanwise mean of q over interior k, per interior (i, j) row
+// (SmoothRampSponge.__call__, wmles/smooth_ramp.py:212-216)
+__global__ void sponge_mean_kernel(const __grid_constant__ SpongeArgs S) {
+    const int b = blockIdx.y;
+    const BlockDev& B = S.blocks[b];
+    const int ng = B.ng, ni = B.n[0], nj = B.n[1], nk = B.n[2];
+    const int row = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    if (row >= ni * nj) return;
+    const int lane = threadIdx.x & 31;
+    const int i = row / nj + ng, j = row % nj + ng;
+    const long long N = B.ncell;
+    const long long base = i * B.plane + (long long)j * B.N[2];
+    const double* q = S.q[b];
+    double acc[5] = {0, 0, 0, 0, 0}, vs = 0.0;
+    for (int k = ng + lane; k < ng + nk; k += 32) {
+        const double vol = B.met[WM_MET_VOL * N + base + k];
+        vs += vol;
+#pragma unroll
+        for (int v = 0; v < 5; ++v) acc[v] += q[v * N + base + k] * vol;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        vs += __shfl_down_sync(0xffffffffu, vs, o);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) acc[v] += __shfl_down_sync(0xffffffffu, acc[v], o);
+    }
+    if (lane == 0) {
+        const long long mn = (long long)B.N[0] * B.N[1];
+        const long long mi = (long long)i * B.N[1] + j;
+#pragma unroll
+        for (int v = 0; v < 5; ++v) S.mean[b][v * mn + mi] = acc[v] / vs;
+    }
+}
+
+cudaError_t launch_sponge_mean(const SpongeArgs& S, int max_rows, cudaStream_t s) {
+    dim3 grid((max_rows + 3) / 4, S.nblocks);
+    sponge_mean_kernel<<<grid, 128, 0, s>>>(S);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ synthetic inflow
+// SmoothRampInflow.fill_at_time / _unit_noise (wmles/smooth_ramp.py:150-197): one CTA per
+// (ghost layer, j) row, threads over k.
+constexpr int IN_NT = 256;
+
+__device__ double interp_col(const double* tab, int n, double y, int col) {
+    // np.interp with end clamping on column 0 as abscissa
+    if (y <= tab[0]) return tab[col];
+    if (y >= tab[7 * (n - 1)]) return tab[7 * (n - 1) + col];
+    int lo = 0, hi = n - 1;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (tab[7 * mid] <= y) lo = mid; else hi = mid;
+    }
+    const double x0 = tab[7 * lo], x1 = tab[7 * hi];
+    const double f0 = tab[7 * lo + col], f1 = tab[7 * hi + col];
+    const double slope = (f1 - f0) / (x1 - x0);
+    return slope * (y - x0) + f0;
+}
+
+__global__ void __launch_bounds__(IN_NT) inflow_kernel(const __grid_constant__ InflowArgs I) {
+    extern __shared__ double fsm[];            // 3 x Nk
+    __shared__ double red[IN_NT / 32];
+    const BlockDev& B = *I.block;
+    const int ng = B.ng, Nj = B.N[1], Nk = B.N[2], nk = B.n[2];
+    const int j = blockIdx.x, m = blockIdx.y, gi = ng - 1 - m;
+    const long long N = B.ncell;
+    const double time = I.time0 + I.time_dt * (I.dt ? *I.dt : 0.0);
+    const double X = I.U_inf * time / I.L;
+    double* f0 = fsm;
+    for (int c = 0; c < 3; ++c) {
+        double* f = fsm + c * Nk;
+        const double* kx = I.modes + (c * 4 + 0) * I.n_modes;
+        const double* ky = I.modes + (c * 4 + 1) * I.n_modes;
+        const double* kz = I.modes + (c * 4 + 2) * I.n_modes;
+        const double* ph = I.modes + (c * 4 + 3) * I.n_modes;
+        double s_int = 0.0;
+        for (int k = threadIdx.x; k < Nk; k += IN_NT) {
+            const long long idx = ((long long)gi * Nj + j) * Nk + k;
+            const double y = B.met[WM_MET_XCY * N + idx] / I.L, z = B.met[WM_MET_XCZ * N + idx] / I.L;
+            double acc = 0.0;
+            for (int q = 0; q < I.n_modes; ++q) acc += cos(((kx[q] * X + ky[q] * y) + kz[q] * z) + ph[q]);
+            f[k] = acc;
+            if (k >= ng && k < ng + nk) s_int += acc;
+        }
+        const double mean = block_sum<IN_NT>(s_int, red) / nk;
+        double cov_acc = 0.0;
+        for (int k = threadIdx.x; k < Nk; k += IN_NT) {
+            f[k] -= mean;
+            if (c == 1 && k >= ng && k < ng + nk) cov_acc += f[k] * f0[k];
+        }
+        if (c == 1) {
+            const double cov = block_sum<IN_NT>(cov_acc, red) / nk;
+            for (int k = threadIdx.x; k < Nk; k += IN_NT) f[k] -= cov * f0[k];
+        }
+        double v_acc = 0.0;
+        for (int k = threadIdx.x; k < Nk; k += IN_NT)
+            if (k >= ng && k < ng + nk) v_acc += f[k] * f[k];
+        const double var = block_sum<IN_NT>(v_acc, red) / nk;
+        const double inv = 1.0 / sqrt(fmax(var, 1e-20));
+        for (int k = threadIdx.x; k < Nk; k += IN_NT) f[k] *= inv;
+        __syncthreads();
+    }
+    const long long on = (long long)ng * Nj * Nk;
+    const double U = I.U_inf;
+    for (int k = threadIdx.x; k < Nk; k += IN_NT) {
+        const long long idx = ((long long)gi * Nj + j) * Nk + k;
+        const double y = B.met[WM_MET_XCY * N + idx] / I.L;
+        const double uu = fmax(interp_col(I.table, I.n_tab, y, 3), 0.0) * (U * U);
+        const double vv = fmax(interp_col(I.table, I.n_tab, y, 4), 0.0) * (U * U);
+        const double ww = fmax(interp_col(I.table, I.n_tab, y, 5), 0.0) * (U * U);
+        const double uv = interp_col(I.table, I.n_tab, y, 6) * (U * U);
+        const double su = sqrt(uu);
+        const double l10 = su > 1e-14 ? uv / fmax(su, 1e-14) : 0.0;
+        const double l11 = sqrt(fmax(vv - l10 * l10, 0.0));
+        const double n0 = fsm[k], n1 = fsm[Nk + k], n2 = fsm[2 * Nk + k];
+        const double u = U * interp_col(I.table, I.n_tab, y, 1) + su * n0;
+        const double v = U * interp_col(I.table, I.n_tab, y, 2) + l10 * n0 + l11 * n1;
+        const double w = sqrt(ww) * n2;
+        const double rho = I.rho_inf, p = I.p_inf;
+        I.out[idx] = rho;
+        I.out[on + idx] = rho * u;
+        I.out[2 * on + idx] = rho * v;
+        I.out[3 * on + idx] = rho * w;
+        I.out[4 * on + idx] = p / I.gm1 + 0.5 * rho * ((u * u + v * v) + w * w);
+    }
+}
+
+cudaError_t launch_inflow(const InflowArgs& I, int Nj, int Nk, int ng, cudaStream_t s) {
+    dim3 grid(Nj, ng);
+    const size_t sm = sizeof(double) * 3 * Nk;
+    inflow_kernel<<<grid, IN_NT, sm, s>>>(I);
+    return cudaGetLastError();
+}
+
+}  // namespace wm
