@@ -1,0 +1,316 @@
+"""Benchmark of the wmles explicit RHS + SSP-RK3 step on B200 (Mcell-steps/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (config 2): periodic channel, one 256x128x128 block (4.19M cells), tanh
+stretching beta=2.5, KEP4 + WALE 0.5, equilibrium wall model on both walls (3rd cell),
+constant mass flux, CFL 0.5, Ma_b 0.3, Re_b 20000; seeded log-law IC + 10 % noise.
+A step is the drivers' loop body: dt = max_dt(Q); Q = advance(Q, dt).
+
+value       whole-job Mcell-steps/s, state resident in HBM, FP64 form, CUDA events, max over
+            ranks (N > 1: one replica per GPU, weak scaling, no data-path collective)
+e2e         the same step through the public Solver API with the state in pinned HOST
+            memory: every step copies the state in, steps, copies the new state and dt out
+mixed       the mixed-precision form (FP32 fluxes/gradients/SGS, FP64 state and reductions)
+roofline    the fused stage kernel: algorithmic bytes per launch / mean launch time
+cpu_baseline  the CPU oracle (NumPy float64 restatement of the reference) on a slab of the
+            same workload, one core
+--impl reference  the oracle on the host cores (one process per core, each on its own slab)
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-steps/s"
+CONFIG_NAME = "channel 256x128x128, KEP4 + WALE + wall model + constant mass flux, SSP-RK3"
+N_CFG2 = (256, 128, 128)
+# DRAM bytes per stage-kernel launch per interior cell from one ncu capture of the same
+# kernel (profiles/stage_kernel_channel.md); None until captured
+TRAFFIC_PER_CELL = {"fp64": None, "mixed": None}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)["hbm_gbs"], "measured"
+    return 6650.0, "fallback"
+
+
+def config_dict(extra=None):
+    d = {"workload": CONFIG_NAME, "cells": int(np.prod(N_CFG2)), "grid": list(N_CFG2), "ghost_layers": 3,
+         "scheme": "KEP4", "sgs": "WALE Cw=0.5", "wall_model": "equilibrium (Spalding/Kader), n_match=3",
+         "constraint": "constant mass flux", "cfl": 0.5, "l2": "inputs larger than L2 (state 188 MB + metrics 527 MB)"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.proc = index, None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- our arm
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from wmles_jax_b200 import Solver, _native
+    from wmles_jax_b200.workloads import channel_case, STAGE_BYTES, STEP_BYTES, CMF_BYTES
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    mesh, gas, kw, prim = channel_case(2, n=N_CFG2)
+    cells = int(np.prod(mesh.blocks[0].n))
+    Q0h = [np.ascontiguousarray(gas.prim_to_cons(np.asarray(prim(g.xc), float))) for g in mesh.geoms]
+    K, Wm = args.steps, args.warmup
+
+    def timed(solver, Q, profile=False):
+        for _ in range(Wm):
+            Q, _ = solver.step(Q)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        solver.profile(enable=profile)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local_rank) as clk:
+            e0.record()
+            for _ in range(K):
+                Q, dt = solver.step(Q)
+            e1.record()
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        barrier()
+        return Q, ms, clk
+
+    out = {}
+    s64 = Solver(mesh, gas, **kw)
+    Q = tuple(torch.from_numpy(q).to(dev) for q in Q0h)
+    Q64, ms64, clk = timed(s64, Q, profile=True)
+    st_ms, st_n = s64.profile_read(_native.KIND_STAGE)
+    all_ms, all_n = s64.profile_read(-1)
+    ms64_max = max_over_ranks(ms64)
+    out["fp64"] = dict(ms=ms64_max / K, stage_ms=st_ms / max(st_n, 1), launches=all_n, clk=clk.summary())
+
+    # mixed precision form (same workload and IC)
+    s32 = Solver(mesh, gas, **kw, precision="mixed")
+    Q = tuple(torch.from_numpy(q).to(dev) for q in Q0h)
+    Q32, ms32, clk32 = timed(s32, Q, profile=True)
+    st32_ms, st32_n = s32.profile_read(_native.KIND_STAGE)
+    ms32_max = max_over_ranks(ms32)
+    err = []
+    for c in range(5):
+        a = mesh.blocks[0].interior(Q32[0][c]).double()
+        b = mesh.blocks[0].interior(Q64[0][c]).double()
+        err.append(float(torch.linalg.norm(a - b) / torch.linalg.norm(b)))
+    out["mixed"] = dict(ms=ms32_max / K, stage_ms=st32_ms / max(st32_n, 1), err=max(err), clk=clk32.summary())
+
+    # end to end through the public API with host buffers
+    pinned = [torch.from_numpy(q).pin_memory() for q in Q0h]
+    res = [torch.empty_like(p).pin_memory() for p in pinned]
+    dbuf = [torch.empty_like(p, device=dev) for p in pinned]
+    h2d = sum(p.numel() * 8 for p in pinned)
+    d2h = h2d + 8
+    for _ in range(max(1, Wm)):
+        for d, p in zip(dbuf, pinned):
+            d.copy_(p, non_blocking=True)
+        Qn, dt = s64.step(tuple(dbuf))
+        for r, q in zip(res, Qn):
+            r.copy_(q, non_blocking=True)
+        float(dt)
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(K):
+        for d, p in zip(dbuf, pinned):
+            d.copy_(p, non_blocking=True)
+        Qn, dt = s64.step(tuple(dbuf))
+        for r, q in zip(res, Qn):
+            r.copy_(q, non_blocking=True)
+        float(dt)                                          # the host reads the step's dt
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1)) / K
+    barrier()
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return None
+    hbm, peak_kind = peaks()
+    f = out["fp64"]
+    alg_launch = np.mean(STAGE_BYTES["fp64"]) * cells
+    achieved = alg_launch / (f["stage_ms"] * 1e-3) / 1e9
+    tr = TRAFFIC_PER_CELL["fp64"]
+    line = {
+        "metric": METRIC, "value": cells * world / (f["ms"] * 1e-3) / 1e6, "unit": METRIC, "n_gpus": world,
+        "steps": K, "warmup": Wm, "ms_per_step": f["ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded log-law IC + 10% noise)",
+        "config": config_dict({"parallelism": f"replicas x{world}" if world > 1 else "1 GPU", "form": "fp64"}),
+        "e2e": {"value": cells * world / (e2e_ms * 1e-3) / 1e6, "unit": METRIC, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
+                "path": "Solver.step with the state copied from/to pinned host memory every step"},
+        "gpu_launches": int(f["launches"]),
+        "roofline": {"bound": "hbm", "kernel": "stage_kernel<double,KEP>", "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": achieved / hbm, "peak_source": f"{peak_kind} hbm_gbs",
+                     "traffic": None if tr is None else tr * cells,
+                     "alg_bytes_per_launch": alg_launch, "mean_launch_ms": f["stage_ms"],
+                     "whole_step_frac": (STEP_BYTES["fp64"] + CMF_BYTES) * cells / (f["ms"] * 1e-3) / 1e9 / hbm},
+        "mixed": {"value": cells * world / (out["mixed"]["ms"] * 1e-3) / 1e6, "ms_per_step": out["mixed"]["ms"],
+                  "speedup_vs_fp64": f["ms"] / out["mixed"]["ms"],
+                  "state_rel_l2_vs_fp64_after_steps": out["mixed"]["err"], "steps_compared": K + Wm,
+                  "stage_launch_ms": out["mixed"]["stage_ms"],
+                  "roofline_frac": np.mean(STAGE_BYTES["mixed"]) * cells / (out["mixed"]["stage_ms"] * 1e-3) / 1e9 / hbm},
+        "clocks": f["clk"],
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args.cpu_cells)
+    if dist is not None:
+        dist.destroy_process_group()
+    return line
+
+
+# ----------------------------------------------------------------------------- CPU oracle
+def _oracle_worker(n, steps, warm, seed):
+    """Run the oracle on one slab of the config-2 channel; returns (cells, steps, seconds)."""
+    sys.path.insert(0, ROOT)
+    from wmles_jax_b200.workloads import channel_case
+    from oracle.wmles_oracle import OracleSolver, init_state
+    mesh, gas, kw, prim = channel_case(2, n=n)
+    s = OracleSolver(mesh, gas, **kw)
+    Q = init_state(s, prim)
+    for _ in range(warm):
+        Q = s.advance(Q, s.max_dt(Q))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        Q = s.advance(Q, s.max_dt(Q))
+    return int(np.prod(n)), steps, time.perf_counter() - t0
+
+
+def cpu_baseline(nx=8):
+    n = (nx, N_CFG2[1], N_CFG2[2])
+    cells, steps, sec = _oracle_worker(n, 6, 1, 0)
+    return {"value": cells * steps / sec / 1e6, "unit": METRIC, "cores": 1, "kind": "port",
+            "sample": f"{steps} steps (after 1 warm-up) of a {n[0]}x{n[1]}x{n[2]} x-periodic slab of the "
+                      f"256x128x128 channel, same physics; NumPy float64 oracle, one process"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    import multiprocessing as mp
+    workers = max(1, min(os.cpu_count() or 1, args.max_workers))
+    n = (args.cpu_cells, N_CFG2[1], N_CFG2[2])
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(workers) as pool:
+        res = pool.starmap(_oracle_worker, [(n, args.steps, args.warmup, i) for i in range(workers)])
+    wall = time.perf_counter() - t0
+    cells_steps = sum(c * s for c, s, _ in res)
+    slowest = max(t for _, _, t in res)
+    value = cells_steps / slowest / 1e6
+    sample = (f"{workers} processes, each {args.steps} steps (after {args.warmup} warm-up) of its own "
+              f"{n[0]}x{n[1]}x{n[2]} x-periodic slab of the 256x128x128 channel (same physics); "
+              f"NumPy float64 oracle restating the reference")
+    return {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": slowest / args.steps * 1e3 * (int(np.prod(N_CFG2)) / (
+                cells_steps / args.steps)), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded log-law IC + 10% noise)", "impl": "reference",
+            "config": config_dict({"form": "fp64", "host": "CPU"}),
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": workers, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": wall}
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-cells", type=int, default=8, help="x-cells of the CPU slab sample")
+    ap.add_argument("--max-workers", type=int, default=64)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be at least 3")
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", args.gpus))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+    else:
+        line = run_ours(args, rank, world, local_rank)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -159,6 +159,17 @@ int wm_step(wm_case* c, double* const* q_in, double* const* q_out, double* dt_de
 /* (tau_w, q_w) of every wall-modelled face: out[w] is a device buffer of 2 x nt1 x nt2. */
 int wm_wall_stats(wm_case* c, const double* const* q, double* const* out, void* stream);
 
+/* Launch accounting and device timing of this library's kernels.  kind: WM_KIND_*.
+ * wm_profile_enable(c, 1) resets the counters and starts recording a CUDA event pair around
+ * every launch on the launching stream; wm_profile_read waits for the recorded events and
+ * returns the summed device time (ms) and the launch count of one kind (-1 = all kinds;
+ * launch counts are kept even with timing disabled).  No reference counterpart: this is the
+ * measurement hook of the benchmark. */
+enum { WM_KIND_STAGE = 0, WM_KIND_GHOST = 1, WM_KIND_WALL = 2, WM_KIND_DT = 3, WM_KIND_SOURCE = 4,
+       WM_NKINDS = 5 };
+int wm_profile_enable(wm_case* c, int enable);
+int wm_profile_read(wm_case* c, int kind, double* ms_total, long long* launches);
+
 #ifdef __cplusplus
 }
 #endif

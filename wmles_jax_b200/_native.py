@@ -70,7 +70,10 @@ SIGNATURES = {
     "wm_advance": (C.c_int, [C.c_void_p, PP, PP, c_double_p, C.c_double, C.c_void_p]),
     "wm_step": (C.c_int, [C.c_void_p, PP, PP, c_double_p, C.c_double, C.c_void_p]),
     "wm_wall_stats": (C.c_int, [C.c_void_p, PP, PP, C.c_void_p]),
+    "wm_profile_enable": (C.c_int, [C.c_void_p, C.c_int]),
+    "wm_profile_read": (C.c_int, [C.c_void_p, C.c_int, c_double_p, C.POINTER(C.c_longlong)]),
 }
+KIND_STAGE, KIND_GHOST, KIND_WALL, KIND_DT, KIND_SOURCE = range(5)
 
 _lib = None
 

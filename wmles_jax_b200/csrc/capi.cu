@@ -71,6 +71,12 @@ struct wm_case {
     unsigned* d_counter = nullptr;
     int dt_ctas = 0;
     double Pr13 = 0, Pr3 = 0, kader_beta = 0;
+    // launch accounting / event timing (wm_profile_*)
+    long long nlaunch[WM_NKINDS] = {0, 0, 0, 0, 0};
+    bool prof = false;
+    struct Rec { int kind; cudaEvent_t a, b; };
+    std::vector<Rec> recs;
+    std::vector<cudaEvent_t> pool;
 };
 
 namespace {
@@ -93,6 +99,36 @@ int dev_upload(wm_case* c, T** p, const T* host, size_t count) {
     if (count && host) CK(cudaMemcpy(*p, host, sizeof(T) * count, cudaMemcpyHostToDevice));
     return WM_OK;
 }
+
+cudaEvent_t pool_event(wm_case* c) {
+    if (!c->pool.empty()) {
+        cudaEvent_t e = c->pool.back();
+        c->pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// brackets one launch of `kind`: counts it and, when profiling, records an event pair
+struct LaunchScope {
+    wm_case* c;
+    int kind, slot = -1;
+    cudaStream_t s;
+    LaunchScope(wm_case* c_, int kind_, cudaStream_t s_, int n = 1) : c(c_), kind(kind_), s(s_) {
+        c->nlaunch[kind] += n;
+        if (c->prof) {
+            wm_case::Rec r{kind, pool_event(c), pool_event(c)};
+            cudaEventRecord(r.a, s);
+            c->recs.push_back(r);
+            slot = (int)c->recs.size() - 1;
+        }
+    }
+    ~LaunchScope() {
+        if (slot >= 0) cudaEventRecord(c->recs[slot].b, s);
+    }
+};
 
 int upload_prog(wm_case* c, GhostProg* g, const wm_ghost_program& p) {
     g->count = p.count;
@@ -196,6 +232,7 @@ int fill_inflow(wm_case* c, double time0, double time_dt, const double* dt, cuda
     I.gm1 = c->hc.gm1;
     I.time0 = time0; I.time_dt = time_dt; I.dt = dt;
     I.out = c->inflow_buf;
+    LaunchScope ls(c, WM_KIND_SOURCE, s);
     CK(launch_inflow(I, B.N[1], B.N[2], B.ng, s));
     return WM_OK;
 }
@@ -205,19 +242,24 @@ int run_stage(wm_case* c, int stage, double* const* q_in, const double* const* q
               const double* dt, double time0, double time_dt, cudaStream_t s) {
     int r;
     if ((r = fill_inflow(c, time0, time_dt, dt, s))) return r;
-    CK(launch_ghost(ghost_args(c, c->prog_rhs, q_in, false), s));
+    {
+        LaunchScope ls(c, WM_KIND_GHOST, s, c->prog_rhs.count ? 1 : 0);
+        CK(launch_ghost(ghost_args(c, c->prog_rhs, q_in, false), s));
+    }
     if (!c->hw.empty()) {
         WallArgs W{};
         W.blocks = c->d_blocks; W.cases = c->d_case; W.walls = c->d_walls;
         W.nwalls = (int)c->hw.size(); W.max_faces = c->max_wall_faces;
         W.Pr13 = c->Pr13; W.Pr3 = c->Pr3; W.kader_beta = c->kader_beta;
         for (int b = 0; b < c->nblocks; ++b) W.q[b] = q_in[b];
+        LaunchScope ls(c, WM_KIND_WALL, s);
         CK(launch_wall(W, s));
     }
     if (c->sponge) {
         SpongeArgs S{};
         S.blocks = c->d_blocks; S.nblocks = c->nblocks;
         for (int b = 0; b < c->nblocks; ++b) { S.q[b] = q_in[b]; S.mean[b] = c->spmean[b]; }
+        LaunchScope ls(c, WM_KIND_SOURCE, s);
         CK(launch_sponge_mean(S, c->sponge_rows, s));
     }
     StageArgs A{};
@@ -231,6 +273,7 @@ int run_stage(wm_case* c, int stage, double* const* q_in, const double* const* q
         A.p[b].q_out = q_out[b];
         A.p[b].spmean = c->sponge ? c->spmean[b] : nullptr;
     }
+    LaunchScope ls(c, WM_KIND_STAGE, s);
     CK(launch_stage(A, c->opts, s));
     return WM_OK;
 }
@@ -245,6 +288,7 @@ int run_dt(wm_case* c, double* const* q, bool apply_cmf, bool want_dt, double* d
     D.want_dt = want_dt ? 1 : 0;
     D.dt_part = c->d_dt_part; D.counter = c->d_counter;
     D.dt_out = dt_out ? dt_out : c->d_dt_tmp;
+    LaunchScope ls(c, WM_KIND_DT, s);
     CK(launch_dt(D, s));
     return WM_OK;
 }
@@ -258,6 +302,8 @@ const char* wm_last_error(void) { return g_err.c_str(); }
 
 void wm_case_destroy(wm_case* c) {
     if (!c) return;
+    for (auto& r : c->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    for (cudaEvent_t e : c->pool) cudaEventDestroy(e);
     for (void* p : c->allocs) cudaFree(p);
     delete c;
 }
@@ -411,6 +457,7 @@ int wm_apply_bcs(wm_case* c, double* const* q, double time, void* stream) {
     cudaStream_t s = (cudaStream_t)stream;
     int r;
     if ((r = fill_inflow(c, time, 0.0, nullptr, s))) return r;
+    LaunchScope ls(c, WM_KIND_GHOST, s, c->prog_all.count ? 2 : 0);
     CK(launch_ghost(ghost_args(c, c->prog_all, q, true), s));
     return WM_OK;
 }
@@ -454,11 +501,41 @@ int wm_wall_stats(wm_case* c, const double* const* q, double* const* out, void* 
     W.nwalls = (int)c->hw.size(); W.max_faces = c->max_wall_faces;
     W.Pr13 = c->Pr13; W.Pr3 = c->Pr3; W.kader_beta = c->kader_beta;
     for (int b = 0; b < c->nblocks; ++b) W.q[b] = q[b];
-    CK(launch_wall(W, s));
+    {
+        LaunchScope ls(c, WM_KIND_WALL, s);
+        CK(launch_wall(W, s));
+    }
     for (size_t w = 0; w < c->hw.size(); ++w) {
         const size_t nf = (size_t)c->hw[w].nt1 * c->hw[w].nt2;
         CK(cudaMemcpyAsync(out[w], c->hw[w].tq, sizeof(double) * 2 * nf, cudaMemcpyDeviceToDevice, s));
     }
+    return WM_OK;
+}
+
+int wm_profile_enable(wm_case* c, int enable) {
+    if (!c) return fail(WM_E_INVALID, "null case");
+    for (auto& r : c->recs) { c->pool.push_back(r.a); c->pool.push_back(r.b); }
+    c->recs.clear();
+    for (int k = 0; k < WM_NKINDS; ++k) c->nlaunch[k] = 0;
+    c->prof = enable != 0;
+    return WM_OK;
+}
+
+int wm_profile_read(wm_case* c, int kind, double* ms_total, long long* launches) {
+    if (!c || kind < -1 || kind >= WM_NKINDS) return fail(WM_E_INVALID, "bad profile query");
+    double ms = 0.0;
+    for (auto& r : c->recs) {
+        if (kind >= 0 && r.kind != kind) continue;
+        CK(cudaEventSynchronize(r.b));
+        float t = 0.f;
+        CK(cudaEventElapsedTime(&t, r.a, r.b));
+        ms += t;
+    }
+    long long n = 0;
+    for (int k = 0; k < WM_NKINDS; ++k)
+        if (kind < 0 || k == kind) n += c->nlaunch[k];
+    if (ms_total) *ms_total = ms;
+    if (launches) *launches = n;
     return WM_OK;
 }
 

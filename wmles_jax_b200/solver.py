@@ -239,6 +239,18 @@ class Solver:
                                   float(time), self._stream()), "wm_step")
         return out, dt
 
+    # ------------------------------------------------------------------ measurement
+    def profile(self, enable=True):
+        """Reset launch counters; with ``enable`` also time every launch with CUDA events."""
+        N.check(self._lib.wm_profile_enable(self._case, 1 if enable else 0), "wm_profile_enable")
+
+    def profile_read(self, kind=-1):
+        """(device ms summed over recorded launches, launch count) of one kernel kind
+        (_native.KIND_*; -1 = all)."""
+        ms, n = C.c_double(), C.c_longlong()
+        N.check(self._lib.wm_profile_read(self._case, int(kind), C.byref(ms), C.byref(n)), "wm_profile_read")
+        return ms.value, n.value
+
     def wall_stats(self, Q):
         """{(block, face): (tau_w, q_w)} host arrays for every wall-modelled face
         (wmles/solver.py:163-179)."""
