@@ -65,10 +65,12 @@ class ClockSampler:
         self.index, self.proc = index, None
 
     def __enter__(self):
+        self.lines = []
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            time.sleep(0.5)                              # let the sampler start
         except OSError:
             self.proc = None
         return self
@@ -132,14 +134,14 @@ def run_ours(args, rank, world, local_rank):
     K, Wm = args.steps, args.warmup
 
     def timed(solver, Q, profile=False):
-        for _ in range(Wm):
-            Q, _ = solver.step(Q)
-        torch.cuda.synchronize()
-        barrier()
-        torch.cuda.synchronize()
-        solver.profile(enable=profile)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        with ClockSampler(local_rank) as clk:
+        with ClockSampler(local_rank) as clk:          # sampling covers warm-up + timed steps
+            for _ in range(Wm):
+                Q, _ = solver.step(Q)
+            torch.cuda.synchronize()
+            barrier()
+            torch.cuda.synchronize()
+            solver.profile(enable=profile)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
             for _ in range(K):
                 Q, dt = solver.step(Q)
@@ -292,8 +294,8 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-cells", type=int, default=8, help="x-cells of the CPU slab sample")
