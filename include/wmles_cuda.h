@@ -156,6 +156,13 @@ int wm_advance(wm_case* c, double* const* q_in, double* const* q_out, const doub
 int wm_step(wm_case* c, double* const* q_in, double* const* q_out, double* dt_dev,
             double time, void* stream);
 
+/* One step with a given time step *dt_in (= wm_max_dt(q_in)), fused with the next step's
+ * CFL reduction: after the constraint pass *dt_next = max_dt(q_out).  A driver loop calls
+ * wm_max_dt once, then feeds each call's dt_next to the next call (the reference's loop
+ * examples/channel_wmles.py:124-125 with one reduction pass per step instead of two). */
+int wm_step_fused(wm_case* c, double* const* q_in, double* const* q_out, const double* dt_in,
+                  double* dt_next, double time, void* stream);
+
 /* (tau_w, q_w) of every wall-modelled face: out[w] is a device buffer of 2 x nt1 x nt2. */
 int wm_wall_stats(wm_case* c, const double* const* q, double* const* out, void* stream);
 

@@ -15,7 +15,8 @@ __device__ __forceinline__ long long cell_index(const BlockDev& B, int axis, int
 }
 
 __device__ __forceinline__ double sutherland_d(double T, const CaseDev& C) {
-    return C.mu_ref * pow(T * C.inv_Tref, 1.5) * C.TrefS / (T + C.S_suth);
+    const double x = T * C.inv_Tref;
+    return C.mu_ref * (x * sqrt(x)) * C.TrefS / (T + C.S_suth);
 }
 
 // ------------------------------------------------------------------ wall model

@@ -492,6 +492,19 @@ int wm_step(wm_case* c, double* const* q_in, double* const* q_out, double* dt_de
     return wm_advance(c, q_in, q_out, dt_dev, time, stream);
 }
 
+int wm_step_fused(wm_case* c, double* const* q_in, double* const* q_out, const double* dt_in, double* dt_next,
+                  double time, void* stream) {
+    if (!c || !q_in || !q_out || !dt_in || !dt_next) return fail(WM_E_INVALID, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    int r;
+    double* const* w0 = c->work[0].data();
+    double* const* w1 = c->work[1].data();
+    if ((r = run_stage(c, 1, q_in, q_in, w0, dt_in, time, 0.0, s))) return r;
+    if ((r = run_stage(c, 2, w0, q_in, w1, dt_in, time, 1.0, s))) return r;
+    if ((r = run_stage(c, 3, w1, q_in, q_out, dt_in, time, 0.5, s))) return r;
+    return run_dt(c, q_out, c->hc.cmf_dir >= 0, true, dt_next, s);
+}
+
 int wm_wall_stats(wm_case* c, const double* const* q, double* const* out, void* stream) {
     if (!c || !q || !out) return fail(WM_E_INVALID, "null argument");
     cudaStream_t s = (cudaStream_t)stream;

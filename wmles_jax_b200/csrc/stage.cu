@@ -1,22 +1,29 @@
 // Fused RHS + SSP-RK3 stage kernel.
 //
 // One CTA owns a TJ x TK tile of (j,k) columns of one block and marches along i over a
-// chunk of planes [i0, i1).  Per plane it keeps, in shared memory:
+// chunk of planes [i0, i1).  Shared memory holds
 //   pr[4]  primitive records of planes i-2..i+1 on the tile + 2-cell halo (rolling ring)
+//   qs     the conservative values of plane i+2 on the same footprint, arriving by
+//          cp.async while plane i is being computed
 //   gs     Green-Gauss gradients, mu_eff, k_eff (and the Ducros sensor) of plane i on the
 //          tile + 1-cell halo
 //   fj/fk  the j- and k-face fluxes of plane i
-// and in registers, per column, the i-face flux of the previous face, the j/k flux
-// differences of the previous plane and that plane's gradient record.  Each face flux is
-// evaluated once; each conservative value is read from HBM about once per stage (halo
-// re-reads hit L2).  The epilogue combines the flux divergence with the RK stage and
-// writes the new state; stage 3 also emits per-tile partial sums of rho u V for the
-// constant-mass-flux constraint.
+// and registers, per column, the previous i-face flux, the j/k flux differences of the
+// previous plane and that plane's gradient record.  Per plane there are three phases
+// separated by barriers:
+//   1. primitives of plane i+1 from the staged conservative values
+//   2. gradient records of plane i
+//   3. own i-face flux -> RK epilogue of plane i-1; all j/k faces of plane i (flat loop);
+//      the cp.async of plane i+2 is in flight meanwhile
+// Each face flux is evaluated once; each conservative value is read from HBM about once
+// per stage (halo re-reads hit L2).  Stage 3 also emits per-tile partial sums of
+// rho u V for the constant-mass-flux constraint.
 //
 // Reference: Solver._block_rhs (wmles/solver.py:76-95), green_gauss / viscous_flux /
 // ducros (wmles/viscous.py), schemes (wmles/schemes.py), SGS (wmles/sgs.py), SSP-RK3
 // (wmles/solver.py:110-121).
 #include <cstdio>
+#include <type_traits>
 #include "physics.cuh"
 #include "stage.cuh"
 
@@ -29,9 +36,14 @@ struct StageLayout {
     static constexpr int GJ = TJ + 2, GK = TK + 2, GN = GJ * GK;   // gradients: 1-cell halo
     static constexpr int NGS = (SCHEME == WM_SCHEME_HYBRID) ? 15 : 14;
     static constexpr int FJN = (TJ + 1) * TK, FKN = TJ * (TK + 1);
-    static constexpr size_t body = sizeof(R) * (size_t(4) * PR_N * PN + size_t(NGS) * GN + 5 * (FJN + FKN));
-    static constexpr size_t red_off = (body + 15) / 16 * 16;        // reduction scratch, 16-byte aligned
+    static constexpr size_t qs_off = 0;                                        // double [5][PN]
+    static constexpr size_t pr_off = qs_off + sizeof(double) * 5 * PN;         // R [4][PR_N][PN]
+    static constexpr size_t gs_off = pr_off + sizeof(R) * 4 * PR_N * PN;       // R [NGS][GN]
+    static constexpr size_t fj_off = gs_off + sizeof(R) * NGS * GN;            // R [5][FJN]
+    static constexpr size_t fk_off = fj_off + sizeof(R) * 5 * FJN;             // R [5][FKN]
+    static constexpr size_t red_off = (fk_off + sizeof(R) * 5 * FKN + 15) / 16 * 16;
     static constexpr size_t bytes = red_off + sizeof(double) * 32;
+    static constexpr int MIN_CTAS = (NT <= 128) ? 2 : 1;
 };
 
 // gradient record: g[0..11] = d(u,v,w,T)/d(x,y,z), 12 = mu_eff, 13 = k_eff, 14 = theta
@@ -50,6 +62,14 @@ __device__ __forceinline__ R xdiff(const BlockDev& B, int comp, long long idx, l
     const double* x = B.met + comp * B.ncell;
     return R(__ldg(x + idx) - __ldg(x + idx - off));
 }
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];\n" ::"l"(p)); }
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p)); }
 
 // viscous flux through one face (times area), wmles/viscous.py:28-51.  gL/gR index a
 // gradient record; pl/pr point at primitive records with component stride s.
@@ -113,14 +133,16 @@ __device__ __forceinline__ void face_flux(const StageOpts& o, const Phys<R>& P, 
 }
 
 template <typename R, int SCHEME, int TJ, int TK>
-__global__ void __launch_bounds__(TJ* TK, 1) stage_kernel(const __grid_constant__ StageArgs A, const StageOpts o) {
+__global__ void __launch_bounds__(TJ* TK, (TJ * TK <= 128) ? 2 : 1)
+    stage_kernel(const __grid_constant__ StageArgs A, const StageOpts o) {
     using LY = StageLayout<R, SCHEME, TJ, TK>;
     constexpr int NT = LY::NT, PK = LY::PK, PN = LY::PN, GK = LY::GK, GN = LY::GN, NGS = LY::NGS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    R* pr = reinterpret_cast<R*>(smem_raw);                 // [4][PR_N][PN]
-    R* gs = pr + 4 * PR_N * PN;                             // [NGS][GN]
-    R* fj = gs + NGS * GN;                                  // [5][FJN]
-    R* fk = fj + 5 * LY::FJN;                               // [5][FKN]
+    double* qs = reinterpret_cast<double*>(smem_raw + LY::qs_off);
+    R* pr = reinterpret_cast<R*>(smem_raw + LY::pr_off);
+    R* gs = reinterpret_cast<R*>(smem_raw + LY::gs_off);
+    R* fj = reinterpret_cast<R*>(smem_raw + LY::fj_off);
+    R* fk = reinterpret_cast<R*>(smem_raw + LY::fk_off);
     double* red = reinterpret_cast<double*>(smem_raw + LY::red_off);
 
     const Tile t = A.tiles[blockIdx.x];
@@ -136,17 +158,24 @@ __global__ void __launch_bounds__(TJ* TK, 1) stage_kernel(const __grid_constant_
     const bool active = (j < jhi) && (k < khi);
     const int sgs_model = o.sgs;
 
-    // ---- load plane ip into ring slot: primitive records on the tile + 2-cell halo
-    auto load_plane = [&](int ip, int slot) {
-        R* dst = pr + slot * PR_N * PN;
+    // ---- conservative values of plane ip on the tile + 2-cell halo -> staging buffer (async)
+    auto stage_plane = [&](int ip) {
         for (int c = tid; c < PN; c += NT) {
             const int jj = c / PK, kk = c - jj * PK;
             const int gj = min(max(t.j0 - 2 + jj, 0), Nj - 1);
             const int gk = min(max(t.k0 - 2 + kk, 0), Nk - 1);
             const long long idx = ip * plane + (long long)gj * Nk + gk;
+#pragma unroll
+            for (int v = 0; v < 5; ++v) cp_async8(qs + v * PN + c, SP.q_in + v * ncell + idx);
+        }
+    };
+    // ---- staged values -> primitive records in ring slot
+    auto convert_plane = [&](int slot) {
+        R* dst = pr + slot * PR_N * PN;
+        for (int c = tid; c < PN; c += NT) {
             double q[5];
 #pragma unroll
-            for (int v = 0; v < 5; ++v) q[v] = __ldg(SP.q_in + v * ncell + idx);
+            for (int v = 0; v < 5; ++v) q[v] = qs[v * PN + c];
             R rec[PR_N];
             cons_to_rec(q, P, rec);
 #pragma unroll
@@ -155,69 +184,46 @@ __global__ void __launch_bounds__(TJ* TK, 1) stage_kernel(const __grid_constant_
     };
 
     // ---- gradient records of plane ip (ring slots of ip-1, ip, ip+1) on the tile + 1-cell halo
-    auto grad_plane = [&](int ip, int sm, int s0, int sp) {
-        const R* Pm = pr + sm * PR_N * PN;
-        const R* P0 = pr + s0 * PR_N * PN;
-        const R* Pp = pr + sp * PR_N * PN;
+    auto grad_plane = [&](int ip) {
+        const R* Pm = pr + ((ip - 1) & 3) * PR_N * PN;
+        const R* P0 = pr + (ip & 3) * PR_N * PN;
+        const R* Pp = pr + ((ip + 1) & 3) * PR_N * PN;
         for (int c = tid; c < GN; c += NT) {
             const int jj = c / GK, kk = c - jj * GK;
             const int pc = (jj + 1) * PK + (kk + 1);
             const int gj = min(t.j0 - 1 + jj, Nj - 2), gk = min(t.k0 - 1 + kk, Nk - 2);
             const long long idx = ip * plane + (long long)gj * Nk + gk;
             const int pv[4] = {PR_U, PR_V, PR_W, PR_T};
+            // metrics first: their loads overlap
+            const R Six = met<R>(B, WM_MET_SIX, idx), Siy = met<R>(B, WM_MET_SIY, idx), Siz = met<R>(B, WM_MET_SIZ, idx);
+            const R Hix = met<R>(B, WM_MET_SIX, idx + plane), Hiy = met<R>(B, WM_MET_SIY, idx + plane),
+                    Hiz = met<R>(B, WM_MET_SIZ, idx + plane);
+            const R Sjx = met<R>(B, WM_MET_SJX, idx), Sjy = met<R>(B, WM_MET_SJY, idx), Sjz = met<R>(B, WM_MET_SJZ, idx);
+            const R Hjx = met<R>(B, WM_MET_SJX, idx + Nk), Hjy = met<R>(B, WM_MET_SJY, idx + Nk),
+                    Hjz = met<R>(B, WM_MET_SJZ, idx + Nk);
+            const R Skx = met<R>(B, WM_MET_SKX, idx), Sky = met<R>(B, WM_MET_SKY, idx), Skz = met<R>(B, WM_MET_SKZ, idx);
+            const R Hkx = met<R>(B, WM_MET_SKX, idx + 1), Hky = met<R>(B, WM_MET_SKY, idx + 1),
+                    Hkz = met<R>(B, WM_MET_SKZ, idx + 1);
+            const R vol = met<R>(B, WM_MET_VOL, idx);
+            const R delta = sgs_model != WM_SGS_NONE ? met<R>(B, WM_MET_DELTA, idx) : R(0);
             R acc[12];
 #pragma unroll
-            for (int q = 0; q < 12; ++q) acc[q] = R(0);
-            // direction 0 (i): neighbours in the ring
-            {
-                const R Slx = met<R>(B, WM_MET_SIX, idx), Sly = met<R>(B, WM_MET_SIY, idx), Slz = met<R>(B, WM_MET_SIZ, idx);
-                const R Shx = met<R>(B, WM_MET_SIX, idx + plane), Shy = met<R>(B, WM_MET_SIY, idx + plane),
-                        Shz = met<R>(B, WM_MET_SIZ, idx + plane);
-#pragma unroll
-                for (int a = 0; a < 4; ++a) {
-                    const R c0 = P0[pv[a] * PN + pc];
-                    const R lo = R(0.5) * (Pm[pv[a] * PN + pc] + c0), hi = R(0.5) * (c0 + Pp[pv[a] * PN + pc]);
-                    acc[3 * a] += hi * Shx - lo * Slx;
-                    acc[3 * a + 1] += hi * Shy - lo * Sly;
-                    acc[3 * a + 2] += hi * Shz - lo * Slz;
-                }
+            for (int a = 0; a < 4; ++a) {
+                const R c0 = P0[pv[a] * PN + pc];
+                const R li = R(0.5) * (Pm[pv[a] * PN + pc] + c0), hi = R(0.5) * (c0 + Pp[pv[a] * PN + pc]);
+                const R lj = R(0.5) * (P0[pv[a] * PN + pc - PK] + c0), hj = R(0.5) * (c0 + P0[pv[a] * PN + pc + PK]);
+                const R lk = R(0.5) * (P0[pv[a] * PN + pc - 1] + c0), hk = R(0.5) * (c0 + P0[pv[a] * PN + pc + 1]);
+                acc[3 * a] = ((hi * Hix - li * Six) + (hj * Hjx - lj * Sjx)) + (hk * Hkx - lk * Skx);
+                acc[3 * a + 1] = ((hi * Hiy - li * Siy) + (hj * Hjy - lj * Sjy)) + (hk * Hky - lk * Sky);
+                acc[3 * a + 2] = ((hi * Hiz - li * Siz) + (hj * Hjz - lj * Sjz)) + (hk * Hkz - lk * Skz);
             }
-            // direction 1 (j)
-            {
-                const R Slx = met<R>(B, WM_MET_SJX, idx), Sly = met<R>(B, WM_MET_SJY, idx), Slz = met<R>(B, WM_MET_SJZ, idx);
-                const R Shx = met<R>(B, WM_MET_SJX, idx + Nk), Shy = met<R>(B, WM_MET_SJY, idx + Nk),
-                        Shz = met<R>(B, WM_MET_SJZ, idx + Nk);
-#pragma unroll
-                for (int a = 0; a < 4; ++a) {
-                    const R c0 = P0[pv[a] * PN + pc];
-                    const R lo = R(0.5) * (P0[pv[a] * PN + pc - PK] + c0), hi = R(0.5) * (c0 + P0[pv[a] * PN + pc + PK]);
-                    acc[3 * a] += hi * Shx - lo * Slx;
-                    acc[3 * a + 1] += hi * Shy - lo * Sly;
-                    acc[3 * a + 2] += hi * Shz - lo * Slz;
-                }
-            }
-            // direction 2 (k)
-            {
-                const R Slx = met<R>(B, WM_MET_SKX, idx), Sly = met<R>(B, WM_MET_SKY, idx), Slz = met<R>(B, WM_MET_SKZ, idx);
-                const R Shx = met<R>(B, WM_MET_SKX, idx + 1), Shy = met<R>(B, WM_MET_SKY, idx + 1),
-                        Shz = met<R>(B, WM_MET_SKZ, idx + 1);
-#pragma unroll
-                for (int a = 0; a < 4; ++a) {
-                    const R c0 = P0[pv[a] * PN + pc];
-                    const R lo = R(0.5) * (P0[pv[a] * PN + pc - 1] + c0), hi = R(0.5) * (c0 + P0[pv[a] * PN + pc + 1]);
-                    acc[3 * a] += hi * Shx - lo * Slx;
-                    acc[3 * a + 1] += hi * Shy - lo * Sly;
-                    acc[3 * a + 2] += hi * Shz - lo * Slz;
-                }
-            }
-            const R ivol = R(1) / met<R>(B, WM_MET_VOL, idx);
+            const R ivol = R(1) / vol;
 #pragma unroll
             for (int q = 0; q < 12; ++q) acc[q] *= ivol;
             const R T = P0[PR_T * PN + pc];
             const R mu = sutherland(T, P);
             R mut = R(0);
-            if (sgs_model != WM_SGS_NONE)
-                mut = P0[PR_RHO * PN + pc] * sgs_nut(sgs_model, acc, met<R>(B, WM_MET_DELTA, idx), P.sgs_c);
+            if (sgs_model != WM_SGS_NONE) mut = P0[PR_RHO * PN + pc] * sgs_nut(sgs_model, acc, delta, P.sgs_c);
 #pragma unroll
             for (int q = 0; q < 12; ++q) gs[q * GN + c] = acc[q];
             gs[GS_MU * GN + c] = mu + mut;
@@ -258,13 +264,13 @@ __global__ void __launch_bounds__(TJ* TK, 1) stage_kernel(const __grid_constant_
                              [&](int v) { return gs[v * GN + gc]; }, Sx, Sy, Sz, dx, dy, dz, F);
     };
 
-    // ---- j- and k-face fluxes of plane ip into shared memory
-    auto jk_fluxes = [&](int ip) {
+    // ---- one j- (f < FJN) or k-face flux of plane ip into shared memory
+    auto jk_face = [&](int ip, int f) {
         const R* P0 = pr + (ip & 3) * PR_N * PN;
-        for (int f = tid; f < LY::FJN; f += NT) {
+        R F[5] = {R(0), R(0), R(0), R(0), R(0)};
+        if (f < LY::FJN) {
             const int row = f / TK, kk = f - row * TK;
             const int gj = t.j0 + row, gk = t.k0 + kk;
-            R F[5] = {R(0), R(0), R(0), R(0), R(0)};
             if (gj <= jhi && gk < khi) {
                 bool done = false;
                 if (gj == ng) done = wall_flux(2, ip, gk, F);
@@ -284,11 +290,10 @@ __global__ void __launch_bounds__(TJ* TK, 1) stage_kernel(const __grid_constant_
             }
 #pragma unroll
             for (int v = 0; v < 5; ++v) fj[v * LY::FJN + f] = F[v];
-        }
-        for (int f = tid; f < LY::FKN; f += NT) {
+        } else {
+            f -= LY::FJN;
             const int row = f / (TK + 1), col = f - row * (TK + 1);
             const int gj = t.j0 + row, gk = t.k0 + col;
-            R F[5] = {R(0), R(0), R(0), R(0), R(0)};
             if (gj < jhi && gk <= khi) {
                 bool done = false;
                 if (gk == ng) done = wall_flux(4, ip, gj, F);
@@ -311,6 +316,40 @@ __global__ void __launch_bounds__(TJ* TK, 1) stage_kernel(const __grid_constant_
         }
     };
 
+    // ---- cache-line prefetch of what the next plane reads from global memory: the metrics
+    // of plane ip+1 on the gradient footprint (+1 row/column for upper faces), the i-face
+    // areas of plane ip+2, and (stages 2, 3) the step-start state of plane ip on the tile
+    auto prefetch_next = [&](int ip) {
+        using MT = typename std::conditional<sizeof(R) == 4, float, double>::type;
+        const MT* mbase = sizeof(R) == 4 ? reinterpret_cast<const MT*>(B.met32) : reinterpret_cast<const MT*>(B.met);
+        constexpr int EL = sizeof(MT);
+        constexpr int ROWS = TJ + 3, LINES = ((TK + 3) * EL + 127) / 128 + 1;
+        const int r0 = t.j0 - 1, c0 = t.k0 - 1;
+        const int nmet = WM_NMET + 3;             // 14 components of plane ip+1, S_i of plane ip+2
+        for (int it = tid; it < nmet * ROWS * LINES; it += NT) {
+            const int comp = it / (ROWS * LINES), rem = it - comp * (ROWS * LINES);
+            const int row = rem / LINES, line = rem - row * LINES;
+            const int pl = comp < WM_NMET ? ip + 1 : ip + 2;
+            const int cc = comp < WM_NMET ? comp : comp - WM_NMET;
+            const int gj = min(r0 + row, Nj - 1);
+            if (pl >= B.N[0]) continue;
+            const MT* rowp = mbase + cc * ncell + (long long)pl * plane + (long long)gj * Nk;
+            const uintptr_t a = (reinterpret_cast<uintptr_t>(rowp + c0) & ~uintptr_t(127)) + 128u * line;
+            if (a <= reinterpret_cast<uintptr_t>(rowp + min(c0 + TK + 2, Nk - 1))) prefetch_l1(reinterpret_cast<const void*>(a));
+        }
+        if (A.stage >= 2 && ip < ihi) {
+            constexpr int QL = (TK * 8 + 127) / 128 + 1;
+            for (int it = tid; it < 5 * TJ * QL; it += NT) {
+                const int v = it / (TJ * QL), rem = it - v * (TJ * QL);
+                const int row = rem / QL, line = rem - row * QL;
+                const int gj = min(t.j0 + row, Nj - 1);
+                const double* rowp = SP.q0 + v * ncell + (long long)ip * plane + (long long)gj * Nk;
+                const uintptr_t a = (reinterpret_cast<uintptr_t>(rowp + t.k0) & ~uintptr_t(127)) + 128u * line;
+                if (a <= reinterpret_cast<uintptr_t>(rowp + min(t.k0 + TK - 1, Nk - 1))) prefetch_l2(reinterpret_cast<const void*>(a));
+            }
+        }
+    };
+
     auto save_gs = [&]() {
         const int gc = (tj + 1) * GK + (tk + 1);
 #pragma unroll
@@ -330,86 +369,97 @@ __global__ void __launch_bounds__(TJ* TK, 1) stage_kernel(const __grid_constant_
     const double dt = A.stage ? A.dt[B.case_id] : 0.0;
     double cmf_acc = 0.0;
 
+    // ---- RK epilogue of interior cell (io, j, k): r = -(div F)/V (+ source), stage update
+    auto output = [&](int io, const R Fhi[5]) {
+        const long long idx = io * plane + (long long)j * Nk + k;
+        const R ivol = R(1) / met<R>(B, WM_MET_VOL, idx);
+        R r[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) r[v] = ((-(Fhi[v] - Flo[v]) - dFj[v]) - dFk[v]) * ivol;
+        double rq[5], qi[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) qi[v] = __ldg(SP.q_in + v * ncell + idx);
+        if (C.sponge) {
+            // -sigma(x) (q - spanwise mean), wmles/smooth_ramp.py:212-221
+            const double xl = __ldg(B.met + WM_MET_XCX * ncell + idx) * C.sp_invL;
+            const double eta = fmin(fmax((xl - C.sp_xs) * C.sp_inv_dx, 0.0), 1.0);
+            const double sig = C.sp_sigma0 * (eta * eta * eta * (10.0 + eta * (-15.0 + 6.0 * eta)));
+            const long long mi = (long long)io * Nj + j;
+            const long long mn = (long long)B.N[0] * Nj;
+#pragma unroll
+            for (int v = 0; v < 5; ++v) rq[v] = double(r[v]) - sig * (qi[v] - SP.spmean[v * mn + mi]);
+        } else {
+#pragma unroll
+            for (int v = 0; v < 5; ++v) rq[v] = double(r[v]);
+        }
+        if (A.stage == 0) {
+#pragma unroll
+            for (int v = 0; v < 5; ++v) SP.q_out[v * ncell + idx] = rq[v];
+        } else if (A.stage == 1) {
+#pragma unroll
+            for (int v = 0; v < 5; ++v) SP.q_out[v * ncell + idx] = qi[v] + dt * rq[v];
+        } else if (A.stage == 2) {
+#pragma unroll
+            for (int v = 0; v < 5; ++v)
+                SP.q_out[v * ncell + idx] = 0.75 * __ldg(SP.q0 + v * ncell + idx) + 0.25 * (qi[v] + dt * rq[v]);
+        } else {
+            double qn[5];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                qn[v] = (1.0 / 3.0) * __ldg(SP.q0 + v * ncell + idx) + (2.0 / 3.0) * (qi[v] + dt * rq[v]);
+                SP.q_out[v * ncell + idx] = qn[v];
+            }
+            if (C.cmf_dir >= 0) cmf_acc += qn[1 + C.cmf_dir] * __ldg(B.met + WM_MET_VOL * ncell + idx);
+        }
+    };
+
     // ---- prologue: planes i0-2 .. i0+1, gradients of i0-1 and i0, faces of plane i0
-    load_plane(i0 - 2, (i0 - 2) & 3);
-    load_plane(i0 - 1, (i0 - 1) & 3);
-    load_plane(i0, i0 & 3);
-    load_plane(i0 + 1, (i0 + 1) & 3);
-    __syncthreads();
-    // plane i0-1 needs plane i0-2's ring slot as its lower neighbour
-    grad_plane(i0 - 1, (i0 - 2) & 3, (i0 - 1) & 3, i0 & 3);
+#pragma unroll 1
+    for (int ip = i0 - 2; ip <= i0 + 1; ++ip) {
+        stage_plane(ip);
+        cp_async_wait_all();
+        __syncthreads();
+        convert_plane(ip & 3);
+        __syncthreads();
+    }
+    stage_plane(i0 + 2);                 // in flight during the prologue's compute
+    grad_plane(i0 - 1);
     __syncthreads();
     save_gs();
     __syncthreads();
-    grad_plane(i0, (i0 - 1) & 3, i0 & 3, (i0 + 1) & 3);
+    grad_plane(i0);
     __syncthreads();
     if (active) iface_flux(i0, Flo);
-    jk_fluxes(i0);
+    for (int f = tid; f < LY::FJN + LY::FKN; f += NT) jk_face(i0, f);
+    cp_async_wait_all();
     __syncthreads();
     jk_diff();
     save_gs();
-    __syncthreads();
 
     // ---- march: iteration ip outputs plane ip-1
+#pragma unroll 1
     for (int ip = i0 + 1; ip <= i1; ++ip) {
-        load_plane(ip + 1, (ip + 1) & 3);
+        convert_plane((ip + 1) & 3);     // staged plane ip+1 -> primitives
         __syncthreads();
-        grad_plane(ip, (ip - 1) & 3, ip & 3, (ip + 1) & 3);
+        grad_plane(ip);
         __syncthreads();
-        R Fhi[5];
-        if (active) iface_flux(ip, Fhi);
-        if (ip < i1) jk_fluxes(ip);
+        if (ip + 2 <= i1 + 1) stage_plane(ip + 2);
+        if (ip < i1) prefetch_next(ip);
         if (active) {
-            const int io = ip - 1;
-            const long long idx = io * plane + (long long)j * Nk + k;
-            const R ivol = R(1) / met<R>(B, WM_MET_VOL, idx);
-            R r[5];
-#pragma unroll
-            for (int v = 0; v < 5; ++v) r[v] = ((-(Fhi[v] - Flo[v]) - dFj[v]) - dFk[v]) * ivol;
-            double rq[5], qi[5];
-#pragma unroll
-            for (int v = 0; v < 5; ++v) qi[v] = __ldg(SP.q_in + v * ncell + idx);
-            if (C.sponge) {
-                // -sigma(x) (q - spanwise mean), wmles/smooth_ramp.py:212-221
-                const double xl = __ldg(B.met + WM_MET_XCX * ncell + idx) * C.sp_invL;
-                const double eta = fmin(fmax((xl - C.sp_xs) * C.sp_inv_dx, 0.0), 1.0);
-                const double sig = C.sp_sigma0 * (eta * eta * eta * (10.0 + eta * (-15.0 + 6.0 * eta)));
-                const long long mi = (long long)io * Nj + j;
-                const long long mn = (long long)B.N[0] * Nj;
-#pragma unroll
-                for (int v = 0; v < 5; ++v) rq[v] = double(r[v]) - sig * (qi[v] - SP.spmean[v * mn + mi]);
-            } else {
-#pragma unroll
-                for (int v = 0; v < 5; ++v) rq[v] = double(r[v]);
-            }
-            if (A.stage == 0) {
-#pragma unroll
-                for (int v = 0; v < 5; ++v) SP.q_out[v * ncell + idx] = rq[v];
-            } else if (A.stage == 1) {
-#pragma unroll
-                for (int v = 0; v < 5; ++v) SP.q_out[v * ncell + idx] = qi[v] + dt * rq[v];
-            } else if (A.stage == 2) {
-#pragma unroll
-                for (int v = 0; v < 5; ++v)
-                    SP.q_out[v * ncell + idx] = 0.75 * __ldg(SP.q0 + v * ncell + idx) + 0.25 * (qi[v] + dt * rq[v]);
-            } else {
-                double qn[5];
-#pragma unroll
-                for (int v = 0; v < 5; ++v) {
-                    qn[v] = (1.0 / 3.0) * __ldg(SP.q0 + v * ncell + idx) + (2.0 / 3.0) * (qi[v] + dt * rq[v]);
-                    SP.q_out[v * ncell + idx] = qn[v];
-                }
-                if (C.cmf_dir >= 0) cmf_acc += qn[1 + C.cmf_dir] * __ldg(B.met + WM_MET_VOL * ncell + idx);
-            }
+            R Fhi[5];
+            iface_flux(ip, Fhi);
+            output(ip - 1, Fhi);
 #pragma unroll
             for (int v = 0; v < 5; ++v) Flo[v] = Fhi[v];
         }
+        if (ip < i1)
+            for (int f = tid; f < LY::FJN + LY::FKN; f += NT) jk_face(ip, f);
+        cp_async_wait_all();
         __syncthreads();
         if (ip < i1) {
             jk_diff();
             save_gs();
         }
-        __syncthreads();
     }
 
     if (A.stage == 3 && A.cmf_part != nullptr) {
@@ -427,27 +477,46 @@ __global__ void __launch_bounds__(TJ* TK, 1) stage_kernel(const __grid_constant_
 }
 
 template <typename R, int SCHEME, int TJ, int TK>
+static cudaError_t configure_one() {
+    using LY = StageLayout<R, SCHEME, TJ, TK>;
+    static bool done = false;     // per instantiation; the attribute is set once per process
+    if (!done) {
+        cudaError_t e = cudaFuncSetAttribute(stage_kernel<R, SCHEME, TJ, TK>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LY::bytes);
+        if (e != cudaSuccess) return e;
+        done = true;
+    }
+    return cudaSuccess;
+}
+
+template <typename R, int SCHEME, int TJ, int TK>
 static cudaError_t launch_one(const StageArgs& A, const StageOpts& o, cudaStream_t s) {
     using LY = StageLayout<R, SCHEME, TJ, TK>;
-    auto kern = stage_kernel<R, SCHEME, TJ, TK>;
-    static bool configured = false;   // per instantiation; device attribute set once per process
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LY::bytes);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
-    kern<<<A.ntiles, LY::NT, LY::bytes, s>>>(A, o);
+    cudaError_t e = configure_one<R, SCHEME, TJ, TK>();
+    if (e != cudaSuccess) return e;
+    stage_kernel<R, SCHEME, TJ, TK><<<A.ntiles, LY::NT, LY::bytes, s>>>(A, o);
     return cudaGetLastError();
 }
 
 template <typename R, int SCHEME, int TJ, int TK>
 static int occupancy_one() {
     using LY = StageLayout<R, SCHEME, TJ, TK>;
-    auto kern = stage_kernel<R, SCHEME, TJ, TK>;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LY::bytes) != cudaSuccess) return 1;
+    if (configure_one<R, SCHEME, TJ, TK>() != cudaSuccess) return 1;
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, LY::NT, LY::bytes) != cudaSuccess) return 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage_kernel<R, SCHEME, TJ, TK>, LY::NT, LY::bytes) !=
+        cudaSuccess)
+        return 1;
     return n;
+}
+
+// tile shapes: 0 = 8x32 (1 CTA/SM), 1 = 16x16 (1 CTA/SM), 2 = 4x32 (2 CTAs/SM)
+template <typename R, int SCHEME>
+static cudaError_t launch_tile(const StageArgs& A, const StageOpts& o, cudaStream_t s) {
+    switch (o.tile) {
+        case 1: return launch_one<R, SCHEME, 16, 16>(A, o, s);
+        case 2: return launch_one<R, SCHEME, 4, 32>(A, o, s);
+        default: return launch_one<R, SCHEME, 8, 32>(A, o, s);
+    }
 }
 
 template <typename R, int SCHEME>
@@ -474,15 +543,6 @@ int stage_ctas_per_sm(const StageOpts& o) {
     }
 }
 
-template <typename R, int SCHEME>
-static cudaError_t launch_tile(const StageArgs& A, const StageOpts& o, cudaStream_t s) {
-    switch (o.tile) {
-        case 1: return launch_one<R, SCHEME, 16, 16>(A, o, s);
-        case 2: return launch_one<R, SCHEME, 4, 32>(A, o, s);
-        default: return launch_one<R, SCHEME, 8, 32>(A, o, s);
-    }
-}
-
 cudaError_t launch_stage(const StageArgs& A, const StageOpts& o, cudaStream_t s) {
     if (o.precision == WM_PREC_MIXED) {
         switch (o.scheme) {
@@ -504,16 +564,6 @@ void tile_shape(int tile, int* tj, int* tk) {
         case 2: *tj = 4; *tk = 32; break;
         default: *tj = 8; *tk = 32; break;
     }
-}
-
-size_t stage_smem_bytes(int precision, int scheme, int tile) {
-    int tj, tk;
-    tile_shape(tile, &tj, &tk);
-    const size_t rs = precision == WM_PREC_MIXED ? 4 : 8;
-    const int ngs = scheme == WM_SCHEME_HYBRID ? 15 : 14;
-    const size_t body = rs * (size_t(4) * PR_N * (tj + 4) * (tk + 4) + size_t(ngs) * (tj + 2) * (tk + 2) +
-                              5 * ((tj + 1) * tk + tj * (tk + 1)));
-    return (body + 15) / 16 * 16 + sizeof(double) * 32;
 }
 
 }  // namespace wm

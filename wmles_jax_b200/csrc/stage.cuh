@@ -15,7 +15,6 @@ struct StageOpts {
 
 cudaError_t launch_stage(const StageArgs& A, const StageOpts& o, cudaStream_t s);
 void tile_shape(int tile, int* tj, int* tk);
-size_t stage_smem_bytes(int precision, int scheme, int tile);
 int stage_ctas_per_sm(const StageOpts& o);
 
 }  // namespace wm
