@@ -100,21 +100,25 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
     return r;
 }
 
+// min that propagates NaN like NumPy's np.min (a NaN time step must not be masked)
+__device__ __forceinline__ double nanmin(double a, double b) { return (a != a || a < b) ? a : b; }
+
 template <int NT>
 __device__ __forceinline__ double block_min(double v, double* red) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_down_sync(0xffffffffu, v, o));
+    for (int o = 16; o > 0; o >>= 1) v = nanmin(v, __shfl_down_sync(0xffffffffu, v, o));
     __syncthreads();
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
     __syncthreads();
     double m = DBL_MAX;
     if (threadIdx.x == 0)
-        for (int w = 0; w < NT / 32; ++w) m = fmin(m, red[w]);
+        for (int w = 0; w < NT / 32; ++w) m = nanmin(m, red[w]);
     return m;   // valid in thread 0
 }
 
 // CFL time step (Solver._dt, wmles/solver.py:135-151), optionally after applying the
 // constant-mass-flux shift (ConstantMassFlux.__call__, wmles/solver.py:22-36) in place.
+// One interior cell per thread; per-CTA minima, reduced by the last CTA to finish.
 constexpr int DT_NT = 256;
 __global__ void __launch_bounds__(DT_NT) dt_kernel(const __grid_constant__ DtArgs D) {
     __shared__ double red[DT_NT / 32];
@@ -122,22 +126,16 @@ __global__ void __launch_bounds__(DT_NT) dt_kernel(const __grid_constant__ DtArg
     const int b = blockIdx.y;
     const BlockDev& B = D.blocks[b];
     const CaseDev& C = D.cases[B.case_id];
-    const bool cmf = D.cmf_part != nullptr && C.cmf_dir >= 0;
-    double delta = 0.0;
-    if (cmf) {
-        double s = 0.0;
-        for (int i = threadIdx.x; i < D.cmf_nparts; i += DT_NT) s += D.cmf_part[i];
-        s = block_sum<DT_NT>(s, red);
-        delta = C.cmf_target - s / C.cmf_volume;
-    }
-    const int ng = B.ng, ni = B.n[0], nj = B.n[1], nk = B.n[2];
-    const int Nj = B.N[1], Nk = B.N[2];
+    const bool cmf = D.cmf_delta != nullptr && C.cmf_dir >= 0;
+    const int ng = B.ng, nj = B.n[1], nk = B.n[2];
+    const int Nk = B.N[2];
     const long long N = B.ncell, plane = B.plane;
-    const long long ncells = (long long)ni * nj * nk;
-    double* q = D.q[b];
-    const double* met = B.met;
+    const long long ncells = (long long)B.n[0] * nj * nk;
     double dtmin = DBL_MAX;
-    for (long long c = (long long)blockIdx.x * DT_NT + threadIdx.x; c < ncells; c += (long long)gridDim.x * DT_NT) {
+    const long long c = (long long)blockIdx.x * DT_NT + threadIdx.x;
+    if (c < ncells) {
+        double* q = D.q[b];
+        const double* met = B.met;
         const int i = int(c / ((long long)nj * nk)) + ng;
         const int r = int(c % ((long long)nj * nk));
         const int j = r / nk + ng, k = r % nk + ng;
@@ -145,7 +143,19 @@ __global__ void __launch_bounds__(DT_NT) dt_kernel(const __grid_constant__ DtArg
         double qv[5];
 #pragma unroll
         for (int v = 0; v < 5; ++v) qv[v] = q[v * N + idx];
+        // every metric this cell needs, read-only and issued before any store to q
+        const long long off[3] = {plane, Nk, 1};
+        double Sl[9], Sh[9];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+#pragma unroll
+            for (int x = 0; x < 3; ++x) {
+                Sl[3 * d + x] = __ldg(met + (3 * d + x) * N + idx);
+                Sh[3 * d + x] = __ldg(met + (3 * d + x) * N + idx + off[d]);
+            }
+        const double vol = __ldg(met + WM_MET_VOL * N + idx);
         if (cmf) {
+            const double delta = *D.cmf_delta;
             const int m = 1 + C.cmf_dir;
             const double dE = (2.0 * qv[m] * delta + delta * delta) / (2.0 * qv[0]);
             qv[m] = qv[m] + delta;
@@ -153,27 +163,25 @@ __global__ void __launch_bounds__(DT_NT) dt_kernel(const __grid_constant__ DtArg
             q[m * N + idx] = qv[m];
             q[4 * N + idx] = qv[4];
         }
-        if (!D.want_dt) continue;
-        const double rho = qv[0];
-        const double u = qv[1] / rho, v = qv[2] / rho, w = qv[3] / rho;
-        const double p = C.gm1 * (qv[4] - 0.5 * rho * ((u * u + v * v) + w * w));
-        const double T = p / (rho * C.Rg);
-        const double cs = sqrt(C.gamma * C.Rg * T);
-        const double nu = C.nu_fac * sutherland_d(T, C) / rho;
-        const double vol = met[WM_MET_VOL * N + idx];
-        double lam = 0.0, lamv = 0.0;
-        const long long off[3] = {plane, Nk, 1};
+        if (D.want_dt) {
+            const double rho = qv[0];
+            const double u = qv[1] / rho, v = qv[2] / rho, w = qv[3] / rho;
+            const double p = C.gm1 * (qv[4] - 0.5 * rho * ((u * u + v * v) + w * w));
+            const double T = p / (rho * C.Rg);
+            const double cs = sqrt(C.gamma * C.Rg * T);
+            const double nu = C.nu_fac * sutherland_d(T, C) / rho;
+            double lam = 0.0, lamv = 0.0;
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            const double* S = met + (3 * d) * N;
-            const double sx = 0.5 * (S[idx] + S[idx + off[d]]);
-            const double sy = 0.5 * (S[N + idx] + S[N + idx + off[d]]);
-            const double sz = 0.5 * (S[2 * N + idx] + S[2 * N + idx + off[d]]);
-            const double Sm = sqrt((sx * sx + sy * sy) + sz * sz);
-            lam = lam + fabs((u * sx + v * sy) + w * sz) + cs * Sm;
-            lamv = lamv + nu * (Sm * Sm) / vol;
+            for (int d = 0; d < 3; ++d) {
+                const double sx = 0.5 * (Sl[3 * d] + Sh[3 * d]);
+                const double sy = 0.5 * (Sl[3 * d + 1] + Sh[3 * d + 1]);
+                const double sz = 0.5 * (Sl[3 * d + 2] + Sh[3 * d + 2]);
+                const double Sm = sqrt((sx * sx + sy * sy) + sz * sz);
+                lam = lam + fabs((u * sx + v * sy) + w * sz) + cs * Sm;
+                lamv = lamv + nu * (Sm * Sm) / vol;
+            }
+            dtmin = C.cfl / ((lam + 4.0 * lamv) / vol);
         }
-        dtmin = fmin(dtmin, C.cfl / ((lam + 4.0 * lamv) / vol));
     }
     if (!D.want_dt) return;
     const double m = block_min<DT_NT>(dtmin, red);
@@ -188,7 +196,7 @@ __global__ void __launch_bounds__(DT_NT) dt_kernel(const __grid_constant__ DtArg
     if (last) {
         __threadfence();
         double mm = DBL_MAX;
-        for (int i = threadIdx.x; i < nparts; i += DT_NT) mm = fmin(mm, ((volatile double*)D.dt_part)[i]);
+        for (int i = threadIdx.x; i < nparts; i += DT_NT) mm = nanmin(mm, ((volatile double*)D.dt_part)[i]);
         mm = block_min<DT_NT>(mm, red);
         if (threadIdx.x == 0) {
             D.dt_out[0] = mm;

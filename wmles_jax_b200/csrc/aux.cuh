@@ -38,8 +38,7 @@ struct DtArgs {
     int nblocks;
     int ctas_per_block;
     double* q[WM_MAX_BLOCKS];      // state (modified in place when cmf is applied)
-    const double* cmf_part;        // stage-3 partial sums (null: no constraint to apply)
-    int cmf_nparts;
+    const double* cmf_delta;       // constant-mass-flux shift from stage 3 (null: none)
     int want_dt;                   // 0: constraint only
     double* dt_part;               // per-CTA minima
     unsigned int* counter;         // last-CTA-done counter (reset by the last CTA)

@@ -67,8 +67,8 @@ struct wm_case {
     bool sponge = false;
     std::vector<double*> spmean;
     int sponge_rows = 0;
-    double *d_cmf_part = nullptr, *d_dt_part = nullptr, *d_dt_tmp = nullptr;
-    unsigned* d_counter = nullptr;
+    double *d_cmf_part = nullptr, *d_dt_part = nullptr, *d_dt_tmp = nullptr, *d_cmf_delta = nullptr;
+    unsigned* d_counter = nullptr;       // [0]: CFL reduction, [1]: constant-mass-flux reduction
     int dt_ctas = 0;
     double Pr13 = 0, Pr3 = 0, kader_beta = 0;
     // launch accounting / event timing (wm_profile_*)
@@ -150,6 +150,9 @@ int validate(const wm_case_desc* d) {
     if (d->sgs < 0 || d->sgs > WM_SGS_VREMAN) return fail(WM_E_INVALID, "unknown sgs %d", d->sgs);
     if (d->precision != WM_PREC_FP64 && d->precision != WM_PREC_MIXED)
         return fail(WM_E_INVALID, "unknown precision %d", d->precision);
+    if (d->tile < -1 || d->tile > 3) return fail(WM_E_INVALID, "unknown tile shape %d", d->tile);
+    if (d->tile == 3 && d->precision == WM_PREC_FP64)
+        return fail(WM_E_UNSUPPORTED, "tile 3 (16x32) is built for the mixed form only");
     for (int b = 0; b < d->nblocks; ++b) {
         const wm_block& B = d->blocks[b];
         if (B.ng != 3) return fail(WM_E_UNSUPPORTED, "block %d: ng=%d (this build supports ng=3)", b, B.ng);
@@ -267,6 +270,8 @@ int run_stage(wm_case* c, int stage, double* const* q_in, const double* const* q
     A.tiles = c->d_tiles; A.ntiles = (int)c->tiles.size();
     A.stage = stage; A.dt = dt;
     A.cmf_part = (stage == 3 && c->hc.cmf_dir >= 0) ? c->d_cmf_part : nullptr;
+    A.cmf_counter = c->d_counter + 1;
+    A.cmf_delta = c->d_cmf_delta;
     for (int b = 0; b < c->nblocks; ++b) {
         A.p[b].q_in = q_in[b];
         A.p[b].q0 = q0 ? q0[b] : q_in[b];
@@ -283,8 +288,7 @@ int run_dt(wm_case* c, double* const* q, bool apply_cmf, bool want_dt, double* d
     D.blocks = c->d_blocks; D.cases = c->d_case; D.nblocks = c->nblocks;
     D.ctas_per_block = c->dt_ctas;
     for (int b = 0; b < c->nblocks; ++b) D.q[b] = q[b];
-    D.cmf_part = apply_cmf ? c->d_cmf_part : nullptr;
-    D.cmf_nparts = (int)c->tiles.size();
+    D.cmf_delta = apply_cmf ? c->d_cmf_delta : nullptr;
     D.want_dt = want_dt ? 1 : 0;
     D.dt_part = c->d_dt_part; D.counter = c->d_counter;
     D.dt_out = dt_out ? dt_out : c->d_dt_tmp;
@@ -439,10 +443,13 @@ int wm_case_create(const wm_case_desc* d, wm_case** out) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
     long long maxcells = 0;
     for (const BlockDev& B : c->hb) maxcells = std::max(maxcells, (long long)B.n[0] * B.n[1] * B.n[2]);
-    c->dt_ctas = (int)std::max(1LL, std::min((long long)(4 * sms / std::max(1, d->nblocks)) + 1, (maxcells + 255) / 256));
+    (void)sms;
+    c->dt_ctas = (int)std::max(1LL, (maxcells + 255) / 256);      // one interior cell per thread
     if ((r = dev_alloc(c, &c->d_dt_part, (size_t)c->dt_ctas * d->nblocks))) return bail(r);
-    if ((r = dev_alloc(c, &c->d_counter, 1))) return bail(r);
-    CK(cudaMemset(c->d_counter, 0, sizeof(unsigned)));
+    if ((r = dev_alloc(c, &c->d_counter, 2))) return bail(r);
+    CK(cudaMemset(c->d_counter, 0, 2 * sizeof(unsigned)));
+    if ((r = dev_alloc(c, &c->d_cmf_delta, 1))) return bail(r);
+    CK(cudaMemset(c->d_cmf_delta, 0, sizeof(double)));
     if ((r = dev_alloc(c, &c->d_dt_tmp, 1))) return bail(r);
 
     if ((r = dev_upload(c, &c->d_case, &c->hc, 1))) return bail(r);

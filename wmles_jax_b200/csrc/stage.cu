@@ -29,6 +29,14 @@
 
 namespace wm {
 
+// resident CTAs per SM the register budget is sized for: the FP64 form of the 256-thread
+// tiles needs ~250 registers and 170+ KB of shared memory (one CTA); the float form fits
+// two 256-thread CTAs (<= 128 registers, ~96 KB each), three 128-thread CTAs, or one
+// 512-thread CTA
+constexpr int stage_min_ctas(size_t rsize, int nt) {
+    return rsize == 4 ? (nt <= 128 ? 3 : (nt <= 256 ? 2 : 1)) : (nt <= 128 ? 2 : 1);
+}
+
 template <typename R, int SCHEME, int TJ, int TK>
 struct StageLayout {
     static constexpr int NT = TJ * TK;
@@ -43,7 +51,10 @@ struct StageLayout {
     static constexpr size_t fk_off = fj_off + sizeof(R) * 5 * FJN;             // R [5][FKN]
     static constexpr size_t red_off = (fk_off + sizeof(R) * 5 * FKN + 15) / 16 * 16;
     static constexpr size_t bytes = red_off + sizeof(double) * 32;
-    static constexpr int MIN_CTAS = (NT <= 128) ? 2 : 1;
+    // resident CTAs per SM the register budget is sized for: the FP64 form of the 256-thread
+    // tiles needs ~250 registers and 170+ KB of shared memory (one CTA); the float form
+    // fits two 256-thread CTAs (<= 128 registers, ~96 KB each) or three 128-thread CTAs
+    static constexpr int MIN_CTAS = stage_min_ctas(sizeof(R), NT);
 };
 
 // gradient record: g[0..11] = d(u,v,w,T)/d(x,y,z), 12 = mu_eff, 13 = k_eff, 14 = theta
@@ -133,7 +144,7 @@ __device__ __forceinline__ void face_flux(const StageOpts& o, const Phys<R>& P, 
 }
 
 template <typename R, int SCHEME, int TJ, int TK>
-__global__ void __launch_bounds__(TJ* TK, (TJ * TK <= 128) ? 2 : 1)
+__global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
     stage_kernel(const __grid_constant__ StageArgs A, const StageOpts o) {
     using LY = StageLayout<R, SCHEME, TJ, TK>;
     constexpr int NT = LY::NT, PK = LY::PK, PN = LY::PN, GK = LY::GK, GN = LY::GN, NGS = LY::NGS;
@@ -468,10 +479,33 @@ __global__ void __launch_bounds__(TJ* TK, (TJ * TK <= 128) ? 2 : 1)
         for (int off = 16; off > 0; off >>= 1) cmf_acc += __shfl_down_sync(0xffffffffu, cmf_acc, off);
         if ((tid & 31) == 0) red[tid >> 5] = cmf_acc;
         __syncthreads();
+        __shared__ bool last;
         if (tid == 0) {
             double s = 0.0;
             for (int w = 0; w < NT / 32; ++w) s += red[w];
             A.cmf_part[blockIdx.x] = s;
+            __threadfence();
+            last = atomicAdd(A.cmf_counter, 1u) == unsigned(gridDim.x - 1);
+        }
+        __syncthreads();
+        if (last) {
+            // the last tile sums the partials in a fixed order (run-to-run deterministic) and
+            // forms the shift delta = target - sum(rho u V) / sum(V), wmles/solver.py:24-29
+            __threadfence();
+            const volatile double* part = A.cmf_part;
+            double s = 0.0;
+            for (int i = tid; i < (int)gridDim.x; i += NT) s += part[i];
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+            __syncthreads();
+            if ((tid & 31) == 0) red[tid >> 5] = s;
+            __syncthreads();
+            if (tid == 0) {
+                double tot = 0.0;
+                for (int w = 0; w < NT / 32; ++w) tot += red[w];
+                A.cmf_delta[0] = C.cmf_target - tot / C.cmf_volume;
+                *A.cmf_counter = 0u;
+            }
         }
     }
 }
@@ -509,12 +543,15 @@ static int occupancy_one() {
     return n;
 }
 
-// tile shapes: 0 = 8x32 (1 CTA/SM), 1 = 16x16 (1 CTA/SM), 2 = 4x32 (2 CTAs/SM)
+// tile shapes: 0 = 8x32, 1 = 16x16, 2 = 4x32, 3 = 16x32 (float only)
 template <typename R, int SCHEME>
 static cudaError_t launch_tile(const StageArgs& A, const StageOpts& o, cudaStream_t s) {
     switch (o.tile) {
         case 1: return launch_one<R, SCHEME, 16, 16>(A, o, s);
         case 2: return launch_one<R, SCHEME, 4, 32>(A, o, s);
+        case 3:
+            if constexpr (sizeof(R) == 4) return launch_one<R, SCHEME, 16, 32>(A, o, s);
+            else return cudaErrorInvalidValue;     // the FP64 16x32 tile exceeds shared memory
         default: return launch_one<R, SCHEME, 8, 32>(A, o, s);
     }
 }
@@ -524,6 +561,9 @@ static int occupancy_tile(int tile) {
     switch (tile) {
         case 1: return occupancy_one<R, SCHEME, 16, 16>();
         case 2: return occupancy_one<R, SCHEME, 4, 32>();
+        case 3:
+            if constexpr (sizeof(R) == 4) return occupancy_one<R, SCHEME, 16, 32>();
+            else return 0;
         default: return occupancy_one<R, SCHEME, 8, 32>();
     }
 }
@@ -562,6 +602,7 @@ void tile_shape(int tile, int* tj, int* tk) {
     switch (tile) {
         case 1: *tj = 16; *tk = 16; break;
         case 2: *tj = 4; *tk = 32; break;
+        case 3: *tj = 16; *tk = 32; break;
         default: *tj = 8; *tk = 32; break;
     }
 }

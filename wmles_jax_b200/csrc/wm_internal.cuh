@@ -63,6 +63,8 @@ struct StageArgs {
     int stage;              // 0: q_out = RHS; 1,2,3: SSP-RK3 stage
     const double* dt;       // device time step (per case: dt[case_id])
     double* cmf_part;       // stage 3 with constant mass flux: per-tile partial sums
+    unsigned int* cmf_counter;  // last-CTA-done counter (the last CTA resets it)
+    double* cmf_delta;      // constant-mass-flux shift, written by the last CTA
     StatePtrs p[WM_MAX_BLOCKS];
 };
 
