@@ -163,6 +163,21 @@ int wm_step(wm_case* c, double* const* q_in, double* const* q_out, double* dt_de
 int wm_step_fused(wm_case* c, double* const* q_in, double* const* q_out, const double* dt_in,
                   double* dt_next, double time, void* stream);
 
+/* CFL time step of a multiblock state with no device allocation (no counterpart in the
+ * reference: it exists for callers that cannot allocate device memory, e.g. code running
+ * inside another framework's memory pool or a fixed device-memory budget, and it needs no
+ * wm_case).  dims: 4 ints per block (ni, nj, nk, ng); q[b], metrics[b]: device arrays of
+ * block b ((5, Ni, Nj, Nk) state, (WM_NMET, Ni, Nj, Nk) metrics, see WM_MET_*); dt_dev:
+ * device double.  Its reduction scratch is a file-scope static device array of
+ * WM_NOALLOC_MAX_PARTIALS slots (one per 256 interior cells, so at most
+ * WM_NOALLOC_MAX_PARTIALS * 256 interior cells in total; larger inputs are rejected with
+ * WM_E_INVALID).  The first call on a device looks the array up (cudaGetSymbolAddress), so
+ * make it before any stream capture.  All calls share the array: calls that overlap on the
+ * GPU race and must be serialised by the caller. */
+#define WM_NOALLOC_MAX_PARTIALS 32768
+int wm_max_dt_noalloc(int nblocks, const int* dims, const double* const* q, const double* const* metrics,
+                      const wm_gas* gas, double cfl, double* dt_dev, void* stream);
+
 /* (tau_w, q_w) of every wall-modelled face: out[w] is a device buffer of 2 x nt1 x nt2. */
 int wm_wall_stats(wm_case* c, const double* const* q, double* const* out, void* stream);
 

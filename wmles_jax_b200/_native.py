@@ -70,6 +70,8 @@ SIGNATURES = {
     "wm_advance": (C.c_int, [C.c_void_p, PP, PP, c_double_p, C.c_double, C.c_void_p]),
     "wm_step": (C.c_int, [C.c_void_p, PP, PP, c_double_p, C.c_double, C.c_void_p]),
     "wm_step_fused": (C.c_int, [C.c_void_p, PP, PP, c_double_p, c_double_p, C.c_double, C.c_void_p]),
+    "wm_max_dt_noalloc": (C.c_int, [C.c_int, c_int_p, PP, PP, C.POINTER(WmGas), C.c_double, c_double_p,
+                                    C.c_void_p]),
     "wm_wall_stats": (C.c_int, [C.c_void_p, PP, PP, C.c_void_p]),
     "wm_profile_enable": (C.c_int, [C.c_void_p, C.c_int]),
     "wm_profile_read": (C.c_int, [C.c_void_p, C.c_int, c_double_p, C.POINTER(C.c_longlong)]),

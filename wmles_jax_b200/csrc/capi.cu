@@ -41,6 +41,13 @@ struct GhostProg {
 
 }  // namespace
 
+namespace wm {
+int set_error(int code, const char* msg) {
+    g_err = msg;
+    return code;
+}
+}  // namespace wm
+
 struct wm_case {
     int device = 0;
     int nblocks = 0;

@@ -54,6 +54,9 @@ struct StatePtrs {
     const double* spmean;  // sponge spanwise mean of q_in, 5 x Ni x Nj (or null)
 };
 
+// records the calling thread's error text (read by wm_last_error) and returns `code`
+int set_error(int code, const char* msg);
+
 struct StageArgs {
     const BlockDev* blocks;
     const CaseDev* cases;
