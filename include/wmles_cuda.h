@@ -31,7 +31,7 @@ extern "C" {
 
 #define WM_ABI_VERSION 1
 #define WM_MAX_BLOCKS 96      /* blocks per case (all cases of one batched launch) */
-#define WM_NMET 14            /* metric components per cell, see WM_MET_* */
+#define WM_NMET 27            /* metric components per cell, see WM_MET_* */
 
 /* status codes */
 #define WM_OK 0
@@ -41,11 +41,16 @@ extern "C" {
 #define WM_E_UNSUPPORTED (-4) /* option not built into this library */
 
 /* metric component order (per cell, float64): face area vector of the cell's LOWER face
- * in each direction (the reference's S[d][:, c] for face index c), volume, centre, and
- * the SGS filter width V^(1/3) */
+ * in each direction (the reference's S[d][:, c] for face index c), volume, centre, the SGS
+ * filter width V^(1/3), 1/V, and for the lower face in each direction the unit vector
+ * e = (xc[c] - xc[c-1]) / |.| between the two cell centres and 1/|xc[c] - xc[c-1]| (the
+ * geometry of the viscous face-gradient correction; zero on the first layer) */
 enum { WM_MET_SIX = 0, WM_MET_SIY, WM_MET_SIZ, WM_MET_SJX, WM_MET_SJY, WM_MET_SJZ,
        WM_MET_SKX, WM_MET_SKY, WM_MET_SKZ, WM_MET_VOL, WM_MET_XCX, WM_MET_XCY, WM_MET_XCZ,
-       WM_MET_DELTA };
+       WM_MET_DELTA, WM_MET_IVOL,
+       WM_MET_EIX, WM_MET_EIY, WM_MET_EIZ, WM_MET_IDI,
+       WM_MET_EJX, WM_MET_EJY, WM_MET_EJZ, WM_MET_IDJ,
+       WM_MET_EKX, WM_MET_EKY, WM_MET_EKZ, WM_MET_IDK };
 
 enum { WM_SCHEME_KEP = 0, WM_SCHEME_MUSCL = 1, WM_SCHEME_HYBRID = 2 };
 enum { WM_LIMITER_ALBADA = 0, WM_LIMITER_MINMOD = 1 };

@@ -101,7 +101,7 @@ def test_metric_packing(W):
     for blk, g in zip(mesh.blocks, mesh.geoms):
         M = block_metrics(blk, g)
         Ni, Nj, Nk = blk.N
-        assert M.shape == (14,) + blk.N
+        assert M.shape == (27,) + blk.N
         assert np.array_equal(M[0:3], g.S[0][:, :Ni])
         assert np.array_equal(M[5], g.S[1][2, :, :Nj])
         assert np.array_equal(M[13], g.vol ** (1.0 / 3.0))

@@ -165,11 +165,12 @@ __global__ void __launch_bounds__(DT_NT) dt_kernel(const __grid_constant__ DtArg
         }
         if (D.want_dt) {
             const double rho = qv[0];
-            const double u = qv[1] / rho, v = qv[2] / rho, w = qv[3] / rho;
+            const double ir = 1.0 / rho, ivol = 1.0 / vol;
+            const double u = qv[1] * ir, v = qv[2] * ir, w = qv[3] * ir;
             const double p = C.gm1 * (qv[4] - 0.5 * rho * ((u * u + v * v) + w * w));
-            const double T = p / (rho * C.Rg);
+            const double T = p * ir * C.inv_Rg;
             const double cs = sqrt(C.gamma * C.Rg * T);
-            const double nu = C.nu_fac * sutherland_d(T, C) / rho;
+            const double nu = C.nu_fac * sutherland_d(T, C) * ir;
             double lam = 0.0, lamv = 0.0;
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
@@ -178,9 +179,9 @@ __global__ void __launch_bounds__(DT_NT) dt_kernel(const __grid_constant__ DtArg
                 const double sz = 0.5 * (Sl[3 * d + 2] + Sh[3 * d + 2]);
                 const double Sm = sqrt((sx * sx + sy * sy) + sz * sz);
                 lam = lam + fabs((u * sx + v * sy) + w * sz) + cs * Sm;
-                lamv = lamv + nu * (Sm * Sm) / vol;
+                lamv = lamv + nu * (Sm * Sm) * ivol;
             }
-            dtmin = C.cfl / ((lam + 4.0 * lamv) / vol);
+            dtmin = C.cfl * vol / (lam + 4.0 * lamv);
         }
     }
     if (!D.want_dt) return;

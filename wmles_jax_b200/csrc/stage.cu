@@ -66,14 +66,6 @@ __device__ __forceinline__ R met(const BlockDev& B, int comp, long long idx) {
     else return __ldg(B.met + comp * B.ncell + idx);
 }
 
-// centroid difference xc[idx] - xc[idx - off] from the FP64 coordinates (in the mixed form
-// too: a float difference of nearby large coordinates would lose the spacing)
-template <typename R>
-__device__ __forceinline__ R xdiff(const BlockDev& B, int comp, long long idx, long long off) {
-    const double* x = B.met + comp * B.ncell;
-    return R(__ldg(x + idx) - __ldg(x + idx - off));
-}
-
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
     const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
@@ -83,13 +75,11 @@ __device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefe
 __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p)); }
 
 // viscous flux through one face (times area), wmles/viscous.py:28-51.  gL/gR index a
-// gradient record; pl/pr point at primitive records with component stride s.
+// gradient record; pl/pr point at primitive records with component stride s; (e0, e1, e2)
+// is the unit vector from the L to the R cell centre and idist the inverse distance.
 template <typename R, class GL, class GR>
 __device__ __forceinline__ void viscous_flux(const R* pl, const R* pr, int s, GL gL, GR gR, R Sx, R Sy, R Sz,
-                                             R dx, R dy, R dz, R F[5]) {
-    const R dist = wm_sqrt(dx * dx + dy * dy + dz * dz);
-    const R idist = R(1) / dist;
-    const R e0 = dx * idist, e1 = dy * idist, e2 = dz * idist;
+                                             R e0, R e1, R e2, R idist, R F[5]) {
     R gf[12];
     const int pv[4] = {PR_U, PR_V, PR_W, PR_T};
 #pragma unroll
@@ -121,11 +111,12 @@ __device__ __forceinline__ void viscous_flux(const R* pl, const R* pr, int s, GL
     F[4] -= (uf * ts0 + vf * ts1 + wf * ts2) + kf * dTdn;
 }
 
-// total face flux (inviscid scheme + viscous), S = face area vector, d = xc_R - xc_L
+// total face flux (inviscid scheme + viscous), S = face area vector, e / idist = unit
+// centre-to-centre vector and its inverse length
 template <typename R, int SCHEME, class GL, class GR>
 __device__ __forceinline__ void face_flux(const StageOpts& o, const Phys<R>& P, const R* L2, const R* L,
                                           const R* Rr, const R* R2, int s, GL gL, GR gR, R Sx, R Sy,
-                                          R Sz, R dx, R dy, R dz, R F[5]) {
+                                          R Sz, R e0, R e1, R e2, R idist, R F[5]) {
     if constexpr (SCHEME == WM_SCHEME_KEP) {
         kep_flux(o.kep_order, L2, L, Rr, R2, s, Sx, Sy, Sz, F);
     } else if constexpr (SCHEME == WM_SCHEME_MUSCL) {
@@ -140,7 +131,7 @@ __device__ __forceinline__ void face_flux(const StageOpts& o, const Phys<R>& P, 
 #pragma unroll
         for (int v = 0; v < 5; ++v) F[v] = (sw == R(0)) ? Fc[v] : (sw == R(1)) ? Fu[v] : (R(1) - sw) * Fc[v] + sw * Fu[v];
     }
-    viscous_flux<R>(L, Rr, s, gL, gR, Sx, Sy, Sz, dx, dy, dz, F);
+    viscous_flux<R>(L, Rr, s, gL, gR, Sx, Sy, Sz, e0, e1, e2, idist, F);
 }
 
 template <typename R, int SCHEME, int TJ, int TK>
@@ -215,7 +206,7 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
             const R Skx = met<R>(B, WM_MET_SKX, idx), Sky = met<R>(B, WM_MET_SKY, idx), Skz = met<R>(B, WM_MET_SKZ, idx);
             const R Hkx = met<R>(B, WM_MET_SKX, idx + 1), Hky = met<R>(B, WM_MET_SKY, idx + 1),
                     Hkz = met<R>(B, WM_MET_SKZ, idx + 1);
-            const R vol = met<R>(B, WM_MET_VOL, idx);
+            const R ivol = met<R>(B, WM_MET_IVOL, idx);
             const R delta = sgs_model != WM_SGS_NONE ? met<R>(B, WM_MET_DELTA, idx) : R(0);
             R acc[12];
 #pragma unroll
@@ -228,7 +219,6 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
                 acc[3 * a + 1] = ((hi * Hiy - li * Siy) + (hj * Hjy - lj * Sjy)) + (hk * Hky - lk * Sky);
                 acc[3 * a + 2] = ((hi * Hiz - li * Siz) + (hj * Hjz - lj * Sjz)) + (hk * Hkz - lk * Skz);
             }
-            const R ivol = R(1) / vol;
 #pragma unroll
             for (int q = 0; q < 12; ++q) acc[q] *= ivol;
             const R T = P0[PR_T * PN + pc];
@@ -268,11 +258,10 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
         const R* R2 = pr + ((ip + 1) & 3) * PR_N * PN + pc;
         const long long idx = ip * plane + (long long)j * Nk + k;
         const R Sx = met<R>(B, WM_MET_SIX, idx), Sy = met<R>(B, WM_MET_SIY, idx), Sz = met<R>(B, WM_MET_SIZ, idx);
-        const R dx = xdiff<R>(B, WM_MET_XCX, idx, plane);
-        const R dy = xdiff<R>(B, WM_MET_XCY, idx, plane);
-        const R dz = xdiff<R>(B, WM_MET_XCZ, idx, plane);
+        const R e0 = met<R>(B, WM_MET_EIX, idx), e1 = met<R>(B, WM_MET_EIY, idx), e2 = met<R>(B, WM_MET_EIZ, idx);
+        const R id = met<R>(B, WM_MET_IDI, idx);
         face_flux<R, SCHEME>(o, P, L2, L, Rr, R2, PN, [&](int v) { return gsp[v]; },
-                             [&](int v) { return gs[v * GN + gc]; }, Sx, Sy, Sz, dx, dy, dz, F);
+                             [&](int v) { return gs[v * GN + gc]; }, Sx, Sy, Sz, e0, e1, e2, id, F);
     };
 
     // ---- one j- (f < FJN) or k-face flux of plane ip into shared memory
@@ -291,12 +280,11 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
                     const int gc = (row + 1) * GK + (kk + 1);     // R cell in the gradient tile
                     const long long idx = ip * plane + (long long)gj * Nk + gk;
                     const R Sx = met<R>(B, WM_MET_SJX, idx), Sy = met<R>(B, WM_MET_SJY, idx), Sz = met<R>(B, WM_MET_SJZ, idx);
-                    const R dx = xdiff<R>(B, WM_MET_XCX, idx, Nk);
-                    const R dy = xdiff<R>(B, WM_MET_XCY, idx, Nk);
-                    const R dz = xdiff<R>(B, WM_MET_XCZ, idx, Nk);
+                    const R e0 = met<R>(B, WM_MET_EJX, idx), e1 = met<R>(B, WM_MET_EJY, idx);
+                    const R e2 = met<R>(B, WM_MET_EJZ, idx), id = met<R>(B, WM_MET_IDJ, idx);
                     face_flux<R, SCHEME>(o, P, P0 + pc - 2 * PK, P0 + pc - PK, P0 + pc, P0 + pc + PK, PN,
                                          [&](int v) { return gs[v * GN + gc - GK]; },
-                                         [&](int v) { return gs[v * GN + gc]; }, Sx, Sy, Sz, dx, dy, dz, F);
+                                         [&](int v) { return gs[v * GN + gc]; }, Sx, Sy, Sz, e0, e1, e2, id, F);
                 }
             }
 #pragma unroll
@@ -314,12 +302,11 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
                     const int gc = (row + 1) * GK + (col + 1);
                     const long long idx = ip * plane + (long long)gj * Nk + gk;
                     const R Sx = met<R>(B, WM_MET_SKX, idx), Sy = met<R>(B, WM_MET_SKY, idx), Sz = met<R>(B, WM_MET_SKZ, idx);
-                    const R dx = xdiff<R>(B, WM_MET_XCX, idx, 1);
-                    const R dy = xdiff<R>(B, WM_MET_XCY, idx, 1);
-                    const R dz = xdiff<R>(B, WM_MET_XCZ, idx, 1);
+                    const R e0 = met<R>(B, WM_MET_EKX, idx), e1 = met<R>(B, WM_MET_EKY, idx);
+                    const R e2 = met<R>(B, WM_MET_EKZ, idx), id = met<R>(B, WM_MET_IDK, idx);
                     face_flux<R, SCHEME>(o, P, P0 + pc - 2, P0 + pc - 1, P0 + pc, P0 + pc + 1, PN,
                                          [&](int v) { return gs[v * GN + gc - 1]; },
-                                         [&](int v) { return gs[v * GN + gc]; }, Sx, Sy, Sz, dx, dy, dz, F);
+                                         [&](int v) { return gs[v * GN + gc]; }, Sx, Sy, Sz, e0, e1, e2, id, F);
                 }
             }
 #pragma unroll
@@ -336,12 +323,14 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
         constexpr int EL = sizeof(MT);
         constexpr int ROWS = TJ + 3, LINES = ((TK + 3) * EL + 127) / 128 + 1;
         const int r0 = t.j0 - 1, c0 = t.k0 - 1;
-        const int nmet = WM_NMET + 3;             // 14 components of plane ip+1, S_i of plane ip+2
-        for (int it = tid; it < nmet * ROWS * LINES; it += NT) {
+        // components read by the stage kernel: S (0..8), delta, 1/V, e/idist (13..26) of plane
+        // ip+1 (23), then S_i (0..2) of plane ip+2 (3)
+        constexpr int NPF = 26;
+        for (int it = tid; it < NPF * ROWS * LINES; it += NT) {
             const int comp = it / (ROWS * LINES), rem = it - comp * (ROWS * LINES);
             const int row = rem / LINES, line = rem - row * LINES;
-            const int pl = comp < WM_NMET ? ip + 1 : ip + 2;
-            const int cc = comp < WM_NMET ? comp : comp - WM_NMET;
+            const int pl = comp < 23 ? ip + 1 : ip + 2;
+            const int cc = comp < 9 ? comp : (comp < 23 ? comp + 4 : comp - 23);
             const int gj = min(r0 + row, Nj - 1);
             if (pl >= B.N[0]) continue;
             const MT* rowp = mbase + cc * ncell + (long long)pl * plane + (long long)gj * Nk;
@@ -383,7 +372,7 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
     // ---- RK epilogue of interior cell (io, j, k): r = -(div F)/V (+ source), stage update
     auto output = [&](int io, const R Fhi[5]) {
         const long long idx = io * plane + (long long)j * Nk + k;
-        const R ivol = R(1) / met<R>(B, WM_MET_VOL, idx);
+        const R ivol = met<R>(B, WM_MET_IVOL, idx);
         R r[5];
 #pragma unroll
         for (int v = 0; v < 5; ++v) r[v] = ((-(Fhi[v] - Flo[v]) - dFj[v]) - dFk[v]) * ivol;

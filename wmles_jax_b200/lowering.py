@@ -24,7 +24,7 @@ from .bc import SlipWall, NoSlipWall, Dirichlet, CharacteristicFarfield, Extrapo
 from .mesh import Interface, interface_index_map, sl
 from .smooth_ramp import SmoothRampInflow
 
-NMET = 14
+NMET = 27
 OP_SLIP, OP_NOSLIP, OP_FARFIELD = 1, 2, 3
 SRC_CELL, SRC_INFLOW, SRC_CONST = 0, 1, 2
 _K_INFLOW, _K_CONST, _K_OP = 1, 2, 3
@@ -40,6 +40,16 @@ def block_metrics(blk, geom):
     M[9] = geom.vol
     M[10:13] = geom.xc
     M[13] = geom.vol ** (1.0 / 3.0)
+    M[14] = 1.0 / geom.vol
+    # viscous correction geometry of each cell's lower face: e = dx / |dx|, 1 / |dx| with
+    # dx = xc[c] - xc[c - 1] along d (wmles/viscous.py:35-37); zero on the first layer
+    for d in range(3):
+        base = 15 + 4 * d
+        M[base:base + 4] = 0.0
+        dx = geom.xc[sl(4, d, slice(1, None))] - geom.xc[sl(4, d, slice(None, -1))]
+        dist = np.sqrt(np.sum(dx * dx, axis=0))
+        M[(slice(base, base + 3),) + sl(3, d, slice(1, None))] = dx / dist
+        M[(base + 3,) + sl(3, d, slice(1, None))] = 1.0 / dist
     return M
 
 
