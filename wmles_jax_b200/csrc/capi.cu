@@ -366,6 +366,9 @@ int wm_case_create(const wm_case_desc* d, wm_case** out) {
         B.plane = (long long)B.N[1] * B.N[2];
         B.ncell = B.plane * B.N[0];
         for (int f = 0; f < 6; ++f) B.wall[f] = -1;
+        if (B.ncell * WM_NMET >= (1LL << 31))
+            return bail(fail(WM_E_UNSUPPORTED, "block %d: %lld cells exceed the 32-bit metric index range "
+                             "(split the block)", b, B.ncell));
         double* met = nullptr;
         if ((r = dev_upload(c, &met, src.metrics, (size_t)WM_NMET * B.ncell))) return bail(r);
         B.met = met;

@@ -60,10 +60,11 @@ struct StageLayout {
 // gradient record: g[0..11] = d(u,v,w,T)/d(x,y,z), 12 = mu_eff, 13 = k_eff, 14 = theta
 enum { GS_MU = 12, GS_K = 13, GS_TH = 14 };
 
+// metric component arrays in the compute precision
 template <typename R>
-__device__ __forceinline__ R met(const BlockDev& B, int comp, long long idx) {
-    if constexpr (sizeof(R) == 4) return __ldg(B.met32 + comp * B.ncell + idx);
-    else return __ldg(B.met + comp * B.ncell + idx);
+__device__ __forceinline__ const R* metbase(const BlockDev& B) {
+    if constexpr (sizeof(R) == 4) return B.met32;
+    else return B.met;
 }
 
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
@@ -154,6 +155,10 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
     const StatePtrs SP = A.p[t.blk];
     const int ng = B.ng, Nj = B.N[1], Nk = B.N[2];
     const long long plane = B.plane, ncell = B.ncell;
+    // cell and component offsets fit 32 bits (checked at case creation): one base pointer
+    // per cell, 32-bit offsets per component
+    const int planei = (int)B.plane, nc = (int)B.ncell;
+    const R* MB = metbase<R>(B);
     const int tid = threadIdx.x, tj = tid / TK, tk = tid % TK;
     const int jhi = ng + B.n[1], khi = ng + B.n[2], ihi = ng + B.n[0];
     const int j = t.j0 + tj, k = t.k0 + tk;
@@ -166,9 +171,9 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
             const int jj = c / PK, kk = c - jj * PK;
             const int gj = min(max(t.j0 - 2 + jj, 0), Nj - 1);
             const int gk = min(max(t.k0 - 2 + kk, 0), Nk - 1);
-            const long long idx = ip * plane + (long long)gj * Nk + gk;
+            const int idx = ip * planei + gj * Nk + gk;
 #pragma unroll
-            for (int v = 0; v < 5; ++v) cp_async8(qs + v * PN + c, SP.q_in + v * ncell + idx);
+            for (int v = 0; v < 5; ++v) cp_async8(qs + v * PN + c, SP.q_in + v * nc + idx);
         }
     };
     // ---- staged values -> primitive records in ring slot
@@ -194,20 +199,20 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
             const int jj = c / GK, kk = c - jj * GK;
             const int pc = (jj + 1) * PK + (kk + 1);
             const int gj = min(t.j0 - 1 + jj, Nj - 2), gk = min(t.k0 - 1 + kk, Nk - 2);
-            const long long idx = ip * plane + (long long)gj * Nk + gk;
             const int pv[4] = {PR_U, PR_V, PR_W, PR_T};
             // metrics first: their loads overlap
-            const R Six = met<R>(B, WM_MET_SIX, idx), Siy = met<R>(B, WM_MET_SIY, idx), Siz = met<R>(B, WM_MET_SIZ, idx);
-            const R Hix = met<R>(B, WM_MET_SIX, idx + plane), Hiy = met<R>(B, WM_MET_SIY, idx + plane),
-                    Hiz = met<R>(B, WM_MET_SIZ, idx + plane);
-            const R Sjx = met<R>(B, WM_MET_SJX, idx), Sjy = met<R>(B, WM_MET_SJY, idx), Sjz = met<R>(B, WM_MET_SJZ, idx);
-            const R Hjx = met<R>(B, WM_MET_SJX, idx + Nk), Hjy = met<R>(B, WM_MET_SJY, idx + Nk),
-                    Hjz = met<R>(B, WM_MET_SJZ, idx + Nk);
-            const R Skx = met<R>(B, WM_MET_SKX, idx), Sky = met<R>(B, WM_MET_SKY, idx), Skz = met<R>(B, WM_MET_SKZ, idx);
-            const R Hkx = met<R>(B, WM_MET_SKX, idx + 1), Hky = met<R>(B, WM_MET_SKY, idx + 1),
-                    Hkz = met<R>(B, WM_MET_SKZ, idx + 1);
-            const R ivol = met<R>(B, WM_MET_IVOL, idx);
-            const R delta = sgs_model != WM_SGS_NONE ? met<R>(B, WM_MET_DELTA, idx) : R(0);
+            const R* m = MB + (ip * planei + gj * Nk + gk);
+            const R* mi = m + planei;
+            const R* mj = m + Nk;
+            const R* mk = m + 1;
+            const R Six = __ldg(m + WM_MET_SIX * nc), Siy = __ldg(m + WM_MET_SIY * nc), Siz = __ldg(m + WM_MET_SIZ * nc);
+            const R Hix = __ldg(mi + WM_MET_SIX * nc), Hiy = __ldg(mi + WM_MET_SIY * nc), Hiz = __ldg(mi + WM_MET_SIZ * nc);
+            const R Sjx = __ldg(m + WM_MET_SJX * nc), Sjy = __ldg(m + WM_MET_SJY * nc), Sjz = __ldg(m + WM_MET_SJZ * nc);
+            const R Hjx = __ldg(mj + WM_MET_SJX * nc), Hjy = __ldg(mj + WM_MET_SJY * nc), Hjz = __ldg(mj + WM_MET_SJZ * nc);
+            const R Skx = __ldg(m + WM_MET_SKX * nc), Sky = __ldg(m + WM_MET_SKY * nc), Skz = __ldg(m + WM_MET_SKZ * nc);
+            const R Hkx = __ldg(mk + WM_MET_SKX * nc), Hky = __ldg(mk + WM_MET_SKY * nc), Hkz = __ldg(mk + WM_MET_SKZ * nc);
+            const R ivol = __ldg(m + WM_MET_IVOL * nc);
+            const R delta = sgs_model != WM_SGS_NONE ? __ldg(m + WM_MET_DELTA * nc) : R(0);
             R acc[12];
 #pragma unroll
             for (int a = 0; a < 4; ++a) {
@@ -256,10 +261,10 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
         const R* L = pr + ((ip - 1) & 3) * PR_N * PN + pc;
         const R* Rr = pr + (ip & 3) * PR_N * PN + pc;
         const R* R2 = pr + ((ip + 1) & 3) * PR_N * PN + pc;
-        const long long idx = ip * plane + (long long)j * Nk + k;
-        const R Sx = met<R>(B, WM_MET_SIX, idx), Sy = met<R>(B, WM_MET_SIY, idx), Sz = met<R>(B, WM_MET_SIZ, idx);
-        const R e0 = met<R>(B, WM_MET_EIX, idx), e1 = met<R>(B, WM_MET_EIY, idx), e2 = met<R>(B, WM_MET_EIZ, idx);
-        const R id = met<R>(B, WM_MET_IDI, idx);
+        const R* m = MB + (ip * planei + j * Nk + k);
+        const R Sx = __ldg(m + WM_MET_SIX * nc), Sy = __ldg(m + WM_MET_SIY * nc), Sz = __ldg(m + WM_MET_SIZ * nc);
+        const R e0 = __ldg(m + WM_MET_EIX * nc), e1 = __ldg(m + WM_MET_EIY * nc), e2 = __ldg(m + WM_MET_EIZ * nc);
+        const R id = __ldg(m + WM_MET_IDI * nc);
         face_flux<R, SCHEME>(o, P, L2, L, Rr, R2, PN, [&](int v) { return gsp[v]; },
                              [&](int v) { return gs[v * GN + gc]; }, Sx, Sy, Sz, e0, e1, e2, id, F);
     };
@@ -278,10 +283,10 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
                 if (!done) {
                     const int pc = (row + 2) * PK + (kk + 2);     // R cell in the primitive tile
                     const int gc = (row + 1) * GK + (kk + 1);     // R cell in the gradient tile
-                    const long long idx = ip * plane + (long long)gj * Nk + gk;
-                    const R Sx = met<R>(B, WM_MET_SJX, idx), Sy = met<R>(B, WM_MET_SJY, idx), Sz = met<R>(B, WM_MET_SJZ, idx);
-                    const R e0 = met<R>(B, WM_MET_EJX, idx), e1 = met<R>(B, WM_MET_EJY, idx);
-                    const R e2 = met<R>(B, WM_MET_EJZ, idx), id = met<R>(B, WM_MET_IDJ, idx);
+                    const R* m = MB + (ip * planei + gj * Nk + gk);
+                    const R Sx = __ldg(m + WM_MET_SJX * nc), Sy = __ldg(m + WM_MET_SJY * nc), Sz = __ldg(m + WM_MET_SJZ * nc);
+                    const R e0 = __ldg(m + WM_MET_EJX * nc), e1 = __ldg(m + WM_MET_EJY * nc);
+                    const R e2 = __ldg(m + WM_MET_EJZ * nc), id = __ldg(m + WM_MET_IDJ * nc);
                     face_flux<R, SCHEME>(o, P, P0 + pc - 2 * PK, P0 + pc - PK, P0 + pc, P0 + pc + PK, PN,
                                          [&](int v) { return gs[v * GN + gc - GK]; },
                                          [&](int v) { return gs[v * GN + gc]; }, Sx, Sy, Sz, e0, e1, e2, id, F);
@@ -300,10 +305,10 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
                 if (!done) {
                     const int pc = (row + 2) * PK + (col + 2);
                     const int gc = (row + 1) * GK + (col + 1);
-                    const long long idx = ip * plane + (long long)gj * Nk + gk;
-                    const R Sx = met<R>(B, WM_MET_SKX, idx), Sy = met<R>(B, WM_MET_SKY, idx), Sz = met<R>(B, WM_MET_SKZ, idx);
-                    const R e0 = met<R>(B, WM_MET_EKX, idx), e1 = met<R>(B, WM_MET_EKY, idx);
-                    const R e2 = met<R>(B, WM_MET_EKZ, idx), id = met<R>(B, WM_MET_IDK, idx);
+                    const R* m = MB + (ip * planei + gj * Nk + gk);
+                    const R Sx = __ldg(m + WM_MET_SKX * nc), Sy = __ldg(m + WM_MET_SKY * nc), Sz = __ldg(m + WM_MET_SKZ * nc);
+                    const R e0 = __ldg(m + WM_MET_EKX * nc), e1 = __ldg(m + WM_MET_EKY * nc);
+                    const R e2 = __ldg(m + WM_MET_EKZ * nc), id = __ldg(m + WM_MET_IDK * nc);
                     face_flux<R, SCHEME>(o, P, P0 + pc - 2, P0 + pc - 1, P0 + pc, P0 + pc + 1, PN,
                                          [&](int v) { return gs[v * GN + gc - 1]; },
                                          [&](int v) { return gs[v * GN + gc]; }, Sx, Sy, Sz, e0, e1, e2, id, F);
@@ -371,17 +376,17 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
 
     // ---- RK epilogue of interior cell (io, j, k): r = -(div F)/V (+ source), stage update
     auto output = [&](int io, const R Fhi[5]) {
-        const long long idx = io * plane + (long long)j * Nk + k;
-        const R ivol = met<R>(B, WM_MET_IVOL, idx);
+        const int idx = io * planei + j * Nk + k;
+        const R ivol = __ldg(MB + WM_MET_IVOL * nc + idx);
         R r[5];
 #pragma unroll
         for (int v = 0; v < 5; ++v) r[v] = ((-(Fhi[v] - Flo[v]) - dFj[v]) - dFk[v]) * ivol;
         double rq[5], qi[5];
 #pragma unroll
-        for (int v = 0; v < 5; ++v) qi[v] = __ldg(SP.q_in + v * ncell + idx);
+        for (int v = 0; v < 5; ++v) qi[v] = __ldg(SP.q_in + v * nc + idx);
         if (C.sponge) {
             // -sigma(x) (q - spanwise mean), wmles/smooth_ramp.py:212-221
-            const double xl = __ldg(B.met + WM_MET_XCX * ncell + idx) * C.sp_invL;
+            const double xl = __ldg(B.met + WM_MET_XCX * nc + idx) * C.sp_invL;
             const double eta = fmin(fmax((xl - C.sp_xs) * C.sp_inv_dx, 0.0), 1.0);
             const double sig = C.sp_sigma0 * (eta * eta * eta * (10.0 + eta * (-15.0 + 6.0 * eta)));
             const long long mi = (long long)io * Nj + j;
@@ -394,22 +399,22 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
         }
         if (A.stage == 0) {
 #pragma unroll
-            for (int v = 0; v < 5; ++v) SP.q_out[v * ncell + idx] = rq[v];
+            for (int v = 0; v < 5; ++v) SP.q_out[v * nc + idx] = rq[v];
         } else if (A.stage == 1) {
 #pragma unroll
-            for (int v = 0; v < 5; ++v) SP.q_out[v * ncell + idx] = qi[v] + dt * rq[v];
+            for (int v = 0; v < 5; ++v) SP.q_out[v * nc + idx] = qi[v] + dt * rq[v];
         } else if (A.stage == 2) {
 #pragma unroll
             for (int v = 0; v < 5; ++v)
-                SP.q_out[v * ncell + idx] = 0.75 * __ldg(SP.q0 + v * ncell + idx) + 0.25 * (qi[v] + dt * rq[v]);
+                SP.q_out[v * nc + idx] = 0.75 * __ldg(SP.q0 + v * nc + idx) + 0.25 * (qi[v] + dt * rq[v]);
         } else {
             double qn[5];
 #pragma unroll
             for (int v = 0; v < 5; ++v) {
-                qn[v] = (1.0 / 3.0) * __ldg(SP.q0 + v * ncell + idx) + (2.0 / 3.0) * (qi[v] + dt * rq[v]);
-                SP.q_out[v * ncell + idx] = qn[v];
+                qn[v] = (1.0 / 3.0) * __ldg(SP.q0 + v * nc + idx) + (2.0 / 3.0) * (qi[v] + dt * rq[v]);
+                SP.q_out[v * nc + idx] = qn[v];
             }
-            if (C.cmf_dir >= 0) cmf_acc += qn[1 + C.cmf_dir] * __ldg(B.met + WM_MET_VOL * ncell + idx);
+            if (C.cmf_dir >= 0) cmf_acc += qn[1 + C.cmf_dir] * __ldg(B.met + WM_MET_VOL * nc + idx);
         }
     };
 
