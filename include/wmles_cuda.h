@@ -186,6 +186,28 @@ int wm_max_dt_noalloc(int nblocks, const int* dims, const double* const* q, cons
 /* (tau_w, q_w) of every wall-modelled face: out[w] is a device buffer of 2 x nt1 x nt2. */
 int wm_wall_stats(wm_case* c, const double* const* q, double* const* out, void* stream);
 
+/* Batched stepping of several resident cases (no reference counterpart: the reference
+ * advances one case per Solver).  A wm_batch is a fixed set of cases that share the
+ * precision, scheme, SGS model and tile shape; wm_batch_step advances all of them by one
+ * fused step (as wm_step_fused) with ONE launch per kernel per RK stage, so its launch count
+ * does not grow with the number of cases.  Every per-case reduction (CFL minimum, constant
+ * mass flux) runs over that case's own cells in a fixed order, so a case's result is
+ * bit-identical whether it is stepped alone (wm_step_fused) or in any batch.
+ *   q_in, q_out: per block of the batch, the member cases' blocks in member order;
+ *   dt_in, dt_next: per case, device doubles; times: per case, host doubles.
+ * The batch holds pointers to its members: destroy it before any of them.  A case's own
+ * entries and every batch holding it use the case's work states, so calls that touch one
+ * case must be ordered (one stream, or events).  With no member carrying a synthetic
+ * inflow the launches depend only on the pointers, so a step can be captured in a CUDA
+ * graph and replayed while the same buffers alternate. */
+typedef struct wm_batch wm_batch;
+int wm_batch_create(int ncases, wm_case* const* cases, wm_batch** out);
+void wm_batch_destroy(wm_batch* b);
+int wm_batch_step(wm_batch* b, double* const* q_in, double* const* q_out, const double* const* dt_in,
+                  double* const* dt_next, const double* times, void* stream);
+/* blocks and stage tiles of the batch, and the number of kernel launches of one step */
+int wm_batch_info(wm_batch* b, int* nblocks, int* ntiles, long long* launches_per_step);
+
 /* Launch accounting and device timing of this library's kernels.  kind: WM_KIND_*.
  * wm_profile_enable(c, 1) resets the counters and starts recording a CUDA event pair around
  * every launch on the launching stream; wm_profile_read waits for the recorded events and

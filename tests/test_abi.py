@@ -44,6 +44,11 @@ def test_version_and_error_string_without_gpu(lib):
     # argument validation runs before any device call
     lib.wm_case_create.restype = ctypes.c_int
     assert lib.wm_case_create(None, None) == -1
+    lib.wm_batch_create.restype = ctypes.c_int
+    out = ctypes.c_void_p()
+    assert lib.wm_batch_create(0, None, ctypes.byref(out)) == -1
+    assert lib.wm_batch_create(1, (ctypes.c_void_p * 1)(None), ctypes.byref(out)) == -1
+    assert out.value is None
 
 
 STRUCTS = {"wm_gas": N.WmGas, "wm_block": N.WmBlock, "wm_wall": N.WmWall,

@@ -1,0 +1,97 @@
+"""Batched stepping (wm_batch_step) and the continuous-batching server.
+
+Each case's result must be the same alone (Solver.step, one case per call) and in any mix:
+in a batch with other cases, with staggered arrivals and departures, replayed from CUDA
+graphs, and under an admission budget that keeps only some cases resident.  The per-case
+reductions and stage tiles do not depend on the mix, so the tolerance is zero: interior
+states and time steps are compared bit for bit."""
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+# (Re_tau, Ma_b, grid): uneven grids, Reynolds and Mach numbers
+MIX = [(600.0, 0.3, (16, 16, 16)), (2000.0, 0.15, (24, 16, 16)), (5000.0, 0.45, (16, 24, 16)),
+       (1200.0, 0.2, (32, 16, 24))]
+
+
+def _requests(steps, arrivals):
+    from wmles_jax_b200.serving import Request
+    from wmles_jax_b200.workloads import serving_case
+    out = []
+    for r, ((rt, ma, grid), n, t) in enumerate(zip(MIX, steps, arrivals)):
+        out.append(Request(rid=r, build=(lambda rt=rt, ma=ma, grid=grid, r=r: serving_case(rt, ma, grid, seed=r)),
+                           steps=n, arrival=t, dims=(grid,)))
+    return out
+
+
+def _interior(q):
+    return q[:, 3:-3, 3:-3, 3:-3]
+
+
+def _same(Qa, Qb):
+    return all(torch.equal(_interior(a), _interior(b)) for a, b in zip(Qa, Qb))
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_batch_step_matches_alone(precision):
+    from wmles_jax_b200 import Solver
+    from wmles_jax_b200.serving import Batch, serve_alone
+    steps = 6
+    reqs = _requests([steps] * len(MIX), [0.0] * len(MIX))
+    alone = [serve_alone(r, precision=precision) for r in reqs]
+    solvers, bufs, dts = [], [], []
+    for r in reqs:
+        mesh, gas, kw, prim = r.build()
+        s = Solver(mesh, gas, precision=precision, **kw)
+        q = s.init_state(prim)
+        solvers.append(s)
+        bufs.append([q, tuple(torch.empty_like(x) for x in q)])
+        d = s.max_dt(q)
+        dts.append([d, torch.empty_like(d)])
+    batch = Batch(solvers)
+    assert batch.nblocks == len(MIX)
+    for k in range(steps):
+        p = k % 2
+        batch.step([b[p] for b in bufs], [b[1 - p] for b in bufs], [d[p] for d in dts], [d[1 - p] for d in dts])
+    torch.cuda.synchronize()
+    batch.close()
+    for i, (Q, dt) in enumerate(alone):
+        assert _same(bufs[i][steps % 2], Q), f"case {i}: state differs from the case run alone"
+        assert torch.equal(dts[i][steps % 2], dt), f"case {i}: dt differs"
+
+
+def _check_server(results, reqs, alone):
+    assert sorted(results) == [r.rid for r in reqs]
+    for r, (Q, dt) in zip(reqs, alone):
+        res = results[r.rid]
+        assert res.steps == r.steps
+        assert _same(res.state, Q), f"request {r.rid}: served state differs from the case run alone"
+        assert torch.equal(res.dt, dt)
+        assert res.finished >= res.arrival
+
+
+def test_server_same_alone_and_in_the_mix():
+    from wmles_jax_b200.serving import Server, serve_alone
+    reqs = _requests([12, 20, 7, 15], [0.0, 0.0, 0.3, 0.6])
+    alone = [serve_alone(r) for r in reqs]
+    srv = Server(precision="mixed", graphs=True, graph_after=1)
+    results = srv.run(reqs, timeout=300)
+    _check_server(results, reqs, alone)
+    st = srv.stats
+    assert st["memberships"] >= 2          # cases joined and left while others ran
+    assert st["graph_steps"] > 0 and st["captures"] > 0
+    assert st["p50_s"] is not None and st["p99_s"] >= st["p50_s"]
+
+
+def test_server_admission_budget():
+    from wmles_jax_b200.serving import Server, estimate_bytes, serve_alone
+    reqs = _requests([5, 9, 4, 6], [0.0] * 4)
+    alone = [serve_alone(r) for r in reqs]
+    sizes = sorted(estimate_bytes(r.dims, "mixed") for r in reqs)
+    budget = sizes[-1] + sizes[0]           # never room for more than two of them
+    srv = Server(precision="mixed", graphs=False, budget_bytes=budget)
+    results = srv.run(reqs, timeout=300)
+    _check_server(results, reqs, alone)
+    assert srv.stats["peak_admitted_bytes"] <= budget
+    assert srv.stats["memberships"] >= 3

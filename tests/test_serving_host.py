@@ -1,0 +1,52 @@
+"""Host logic of the serving layer that needs no GPU: admission accounting, the device-byte
+estimate, the seeded request mix and the Re_tau -> Re_b mapping."""
+import numpy as np
+import pytest
+
+from wmles_jax_b200.serving import Admission, estimate_bytes
+from wmles_jax_b200.workloads import SERVING_GRIDS, re_bulk_from_re_tau, serving_requests
+
+
+def test_admission_accounting():
+    a = Admission(1000, max_blocks=3, max_cases=2)
+    assert a.fits(600, 1)
+    a.take(600, 1)
+    assert not a.fits(500, 1)          # bytes
+    assert a.fits(400, 2)
+    a.take(400, 2)
+    assert not a.fits(0, 1)            # blocks and cases
+    a.give(600, 1)
+    assert a.fits(500, 1) and a.peak == 1000 and a.used == 400
+    with pytest.raises(ValueError):
+        a.fits(2000, 1)                # can never be admitted
+    with pytest.raises(ValueError):
+        a.fits(10, 4)
+
+
+def test_estimate_bytes():
+    small, big = estimate_bytes([(48, 48, 48)], "mixed"), estimate_bytes([(192, 96, 96)], "mixed")
+    assert big > small > 0
+    assert estimate_bytes([(48, 48, 48)], "fp64") < small          # no FP32 metric copy
+    # at least the two ping-pong and two work states of 5 float64 per ghosted cell
+    assert small >= 4 * 40 * 54 ** 3
+
+
+def test_re_mapping_inverts_dean():
+    re_tau = np.array([550.0, 1000.0, 5200.0])
+    re_m = 2.0 * re_bulk_from_re_tau(re_tau)
+    np.testing.assert_allclose(0.09 * re_m ** 0.88, re_tau, rtol=1e-12)
+
+
+def test_serving_requests_seeded_mix():
+    a, b = serving_requests(), serving_requests()
+    assert len(a) == 64
+    assert [r.arrival for r in a] == [r.arrival for r in b]
+    assert [r.meta for r in a] == [r.meta for r in b]
+    arr = np.array([r.arrival for r in a])
+    assert np.all(np.diff(arr) > 0) and arr[0] > 0
+    assert 1.0 < arr[-1] < 8.0                       # 64 arrivals at 20 per second
+    for r in a:
+        assert 550.0 <= r.meta["re_tau"] <= 5200.0 and 0.1 <= r.meta["ma_b"] <= 0.5
+        assert r.meta["grid"] in SERVING_GRIDS and r.dims == (r.meta["grid"],) and r.steps == 2000
+    assert len({r.meta["grid"] for r in a}) == len(SERVING_GRIDS)
+    assert serving_requests(seed=1)[0].arrival != a[0].arrival

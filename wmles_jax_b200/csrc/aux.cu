@@ -50,7 +50,7 @@ __global__ void wall_kernel(const __grid_constant__ WallArgs A) {
     const double U = sqrt((up[0] * up[0] + up[1] * up[1]) + up[2] * up[2] + 1e-20);
     // equilibrium model
     const double Um = fmax(U, 1e-8);
-    const double T_w = W.isothermal ? W.T_wall : T_h + A.Pr13 * (Um * Um) / (2.0 * C.cp);
+    const double T_w = W.isothermal ? W.T_wall : T_h + C.Pr13 * (Um * Um) / (2.0 * C.cp);
     const double rho_w = p_h / (C.Rg * T_w);
     const double mu_w = sutherland_d(T_w, C);
     const double ut = spalding_utau(W.kappa, W.ekb, W.n_iter, h, Um, rho_w, mu_w);
@@ -61,8 +61,8 @@ __global__ void wall_kernel(const __grid_constant__ WallArgs A) {
         const double Pr = C.Pr;
         const double yp = fmax(h * ut * rho_w / mu_w, 1e-6);
         const double x = Pr * yp, x2 = x * x;
-        const double Gam = fmax(0.01 * (x2 * x2) / (1.0 + 5.0 * A.Pr3 * yp), 1e-20);
-        const double Tp = Pr * yp * exp(-Gam) + (2.12 * log(1.0 + yp) + A.kader_beta) * exp(-1.0 / Gam);
+        const double Gam = fmax(0.01 * (x2 * x2) / (1.0 + 5.0 * C.Pr3 * yp), 1e-20);
+        const double Tp = Pr * yp * exp(-Gam) + (2.12 * log(1.0 + yp) + C.kader_beta) * exp(-1.0 / Gam);
         qw = rho_w * C.cp * ut * (T_w - T_h) / Tp;
     }
     const double sgn = W.side == 1 ? 1.0 : -1.0;
@@ -118,12 +118,19 @@ __device__ __forceinline__ double block_min(double v, double* red) {
 
 // CFL time step (Solver._dt, wmles/solver.py:135-151), optionally after applying the
 // constant-mass-flux shift (ConstantMassFlux.__call__, wmles/solver.py:22-36) in place.
-// One interior cell per thread; per-CTA minima, reduced by the last CTA to finish.
-constexpr int DT_NT = 256;
+// One interior cell per thread over a flat grid of every block's CTAs; per-CTA minima,
+// reduced per case by the last CTA to finish.
 __global__ void __launch_bounds__(DT_NT) dt_kernel(const __grid_constant__ DtArgs D) {
     __shared__ double red[DT_NT / 32];
     __shared__ bool last;
-    const int b = blockIdx.y;
+    int b = 0;
+    {
+        int hi = D.nblocks - 1;
+        while (b < hi) {             // last block whose first CTA is <= blockIdx.x
+            const int mid = (b + hi + 1) >> 1;
+            if (D.cta_start[mid] <= (int)blockIdx.x) b = mid; else hi = mid - 1;
+        }
+    }
     const BlockDev& B = D.blocks[b];
     const CaseDev& C = D.cases[B.case_id];
     const bool cmf = D.cmf_delta != nullptr && C.cmf_dir >= 0;
@@ -132,7 +139,7 @@ __global__ void __launch_bounds__(DT_NT) dt_kernel(const __grid_constant__ DtArg
     const long long N = B.ncell, plane = B.plane;
     const long long ncells = (long long)B.n[0] * nj * nk;
     double dtmin = DBL_MAX;
-    const long long c = (long long)blockIdx.x * DT_NT + threadIdx.x;
+    const long long c = (long long)((int)blockIdx.x - D.cta_start[b]) * DT_NT + threadIdx.x;
     if (c < ncells) {
         double* q = D.q[b];
         const double* met = B.met;
@@ -155,7 +162,7 @@ __global__ void __launch_bounds__(DT_NT) dt_kernel(const __grid_constant__ DtArg
             }
         const double vol = __ldg(met + WM_MET_VOL * N + idx);
         if (cmf) {
-            const double delta = *D.cmf_delta;
+            const double delta = D.cmf_delta[B.case_id];
             const int m = 1 + C.cmf_dir;
             const double dE = (2.0 * qv[m] * delta + delta * delta) / (2.0 * qv[0]);
             qv[m] = qv[m] + delta;
@@ -186,29 +193,31 @@ __global__ void __launch_bounds__(DT_NT) dt_kernel(const __grid_constant__ DtArg
     }
     if (!D.want_dt) return;
     const double m = block_min<DT_NT>(dtmin, red);
-    const int nparts = D.nblocks * D.ctas_per_block;
     if (threadIdx.x == 0) {
-        D.dt_part[b * D.ctas_per_block + blockIdx.x] = m;
+        D.dt_part[blockIdx.x] = m;
         __threadfence();
         const unsigned prev = atomicAdd(D.counter, 1u);
-        last = (prev == unsigned(nparts - 1));
+        last = (prev == unsigned(D.ncta - 1));
     }
     __syncthreads();
     if (last) {
+        // per case: the minimum over the CTAs of that case's blocks
         __threadfence();
-        double mm = DBL_MAX;
-        for (int i = threadIdx.x; i < nparts; i += DT_NT) mm = nanmin(mm, ((volatile double*)D.dt_part)[i]);
-        mm = block_min<DT_NT>(mm, red);
-        if (threadIdx.x == 0) {
-            D.dt_out[0] = mm;
-            *D.counter = 0u;
+        for (int c = 0; c < D.ncases; ++c) {
+            const int p0 = D.cta_start[D.case_block_start[c]];
+            const int p1 = D.cta_start[D.case_block_start[c + 1]];
+            double mm = DBL_MAX;
+            for (int i = p0 + threadIdx.x; i < p1; i += DT_NT) mm = nanmin(mm, ((volatile double*)D.dt_part)[i]);
+            mm = block_min<DT_NT>(mm, red);
+            if (threadIdx.x == 0 && D.dt_out[c] != nullptr) D.dt_out[c][0] = mm;
+            __syncthreads();
         }
+        if (threadIdx.x == 0) *D.counter = 0u;
     }
 }
 
 cudaError_t launch_dt(const DtArgs& D, cudaStream_t s) {
-    dim3 grid(D.ctas_per_block, D.nblocks);
-    dt_kernel<<<grid, DT_NT, 0, s>>>(D);
+    dt_kernel<<<D.ncta, DT_NT, 0, s>>>(D);
     return cudaGetLastError();
 }
 
@@ -217,6 +226,7 @@ cudaError_t launch_dt(const DtArgs& D, cudaStream_t s) {
 // (SmoothRampSponge.__call__, wmles/smooth_ramp.py:212-216)
 __global__ void sponge_mean_kernel(const __grid_constant__ SpongeArgs S) {
     const int b = blockIdx.y;
+    if (S.mean[b] == nullptr) return;    // block of a case without a sponge
     const BlockDev& B = S.blocks[b];
     const int ng = B.ng, ni = B.n[0], nj = B.n[1], nk = B.n[2];
     const int row = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);

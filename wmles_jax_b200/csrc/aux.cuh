@@ -5,17 +5,10 @@
 namespace wm {
 
 struct GhostArgs {
-    int count;
-    const int* dst;
-    const int* src;
-    const int* ops;
-    const int* op_code;
-    const double* op_nrm;
-    const double* bc;         // 8 per BC
-    const double* inflow;     // 5 x inflow_n (or null)
-    long long inflow_n;
-    double* stash;            // non-null: two-phase gather/scatter (5 x count)
-    double gamma, gm1, Rg;
+    const GhostSeg* segs;     // device table, one segment per case
+    int nseg;
+    int total;                // entries over all segments
+    double* stash;            // non-null: two-phase gather/scatter (5 x total)
     double* q[WM_MAX_BLOCKS];
     long long ncell[WM_MAX_BLOCKS];
 };
@@ -26,23 +19,25 @@ struct WallArgs {
     WallDev* walls;
     int nwalls;
     int max_faces;
-    double Pr13;          // Pr^(1/3)
-    double Pr3;           // Pr^3
-    double kader_beta;    // (3.85 Pr^(1/3) - 1.3)^2 + 2.12 ln Pr
     const double* q[WM_MAX_BLOCKS];
 };
+
+constexpr int DT_NT = 256;   // threads (= interior cells) per CTA of the CFL / constraint pass
 
 struct DtArgs {
     const BlockDev* blocks;
     const CaseDev* cases;
     int nblocks;
-    int ctas_per_block;
-    double* q[WM_MAX_BLOCKS];      // state (modified in place when cmf is applied)
-    const double* cmf_delta;       // constant-mass-flux shift from stage 3 (null: none)
+    int ncta;                              // one CTA per DT_NT interior cells of each block
+    int cta_start[WM_MAX_BLOCKS + 1];      // CTAs of block b: [cta_start[b], cta_start[b+1])
+    int ncases;
+    int case_block_start[MAX_CASES + 1];   // blocks of case c: [start[c], start[c+1])
+    double* q[WM_MAX_BLOCKS];      // state (modified in place when the constraint is applied)
+    const double* cmf_delta;       // per case: constant-mass-flux shift from stage 3 (null: none)
     int want_dt;                   // 0: constraint only
     double* dt_part;               // per-CTA minima
     unsigned int* counter;         // last-CTA-done counter (reset by the last CTA)
-    double* dt_out;                // dt of the case
+    double* dt_out[MAX_CASES];     // per case: time step
 };
 
 struct SpongeArgs {

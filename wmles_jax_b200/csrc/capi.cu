@@ -1,4 +1,14 @@
 // C ABI of libwmles_cuda.so (include/wmles_cuda.h): case set-up and step orchestration.
+//
+// A wm_case owns one case's device data (metrics, ghost programs, wall geometry, work
+// states, inflow/sponge buffers).  Launches run on a View: the concatenated device tables
+// (blocks, per-case constants, wall faces, stage tiles, ghost-program segments) and the
+// reduction scratch of a set of cases.  Every wm_case carries a View of itself for the
+// single-case entry points; a wm_batch is a View over several resident cases, so one
+// launch per kernel and stage advances all of them.  Per-case reductions (CFL minimum,
+// constant-mass-flux sum) run over each case's own CTAs / tiles in a fixed order, so a
+// case's result does not depend on what else is in the batch.
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -39,6 +49,81 @@ struct GhostProg {
     double* op_nrm = nullptr;
 };
 
+// launch accounting / event timing (wm_profile_*)
+struct Prof {
+    long long nlaunch[WM_NKINDS] = {0, 0, 0, 0, 0};
+    bool on = false;
+    struct Rec { int kind; cudaEvent_t a, b; };
+    std::vector<Rec> recs;
+    std::vector<cudaEvent_t> pool;
+
+    cudaEvent_t event() {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void reset(bool enable) {
+        for (auto& r : recs) { pool.push_back(r.a); pool.push_back(r.b); }
+        recs.clear();
+        for (int k = 0; k < WM_NKINDS; ++k) nlaunch[k] = 0;
+        on = enable;
+    }
+    ~Prof() {
+        for (auto& r : recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+        for (cudaEvent_t e : pool) cudaEventDestroy(e);
+    }
+};
+
+// brackets one launch of `kind`: counts it and, when profiling, records an event pair
+struct LaunchScope {
+    Prof* p;
+    int slot = -1;
+    cudaStream_t s;
+    LaunchScope(Prof* p_, int kind, cudaStream_t s_, int n = 1) : p(p_), s(s_) {
+        p->nlaunch[kind] += n;
+        if (p->on && n > 0) {
+            Prof::Rec r{kind, p->event(), p->event()};
+            cudaEventRecord(r.a, s);
+            p->recs.push_back(r);
+            slot = (int)p->recs.size() - 1;
+        }
+    }
+    ~LaunchScope() {
+        if (slot >= 0) cudaEventRecord(p->recs[slot].b, s);
+    }
+};
+
+struct Owner {
+    std::vector<void*> allocs;
+    ~Owner() {
+        for (void* p : allocs) cudaFree(p);
+    }
+    template <typename T>
+    int alloc(T** p, size_t count) {
+        void* v = nullptr;
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc(&v, sizeof(T) * count);
+        if (e != cudaSuccess) return fail(WM_E_CUDA, "cudaMalloc(%zu bytes): %s", sizeof(T) * count, cudaGetErrorString(e));
+        allocs.push_back(v);
+        *p = static_cast<T*>(v);
+        return WM_OK;
+    }
+    template <typename T>
+    int upload(T** p, const T* host, size_t count) {
+        int r = alloc(p, count);
+        if (r) return r;
+        if (count && host) CK(cudaMemcpy(*p, host, sizeof(T) * count, cudaMemcpyHostToDevice));
+        return WM_OK;
+    }
+};
+
+struct View;
+
 }  // namespace
 
 namespace wm {
@@ -50,17 +135,12 @@ int set_error(int code, const char* msg) {
 
 struct wm_case {
     int device = 0;
-    int nblocks = 0;
-    std::vector<BlockDev> hb;           // host copies of the block descriptors
-    std::vector<void*> allocs;
-    BlockDev* d_blocks = nullptr;
+    Owner mem;
+    // host copies of the case-local descriptors (block / wall indices local to the case)
+    std::vector<BlockDev> hb;
     CaseDev hc{};
-    CaseDev* d_case = nullptr;
     std::vector<WallDev> hw;
-    WallDev* d_walls = nullptr;
-    int max_wall_faces = 0;
     std::vector<Tile> tiles;
-    Tile* d_tiles = nullptr;
     StageOpts opts{};
     std::vector<double*> work[2];
     GhostProg prog_rhs, prog_all;
@@ -71,80 +151,47 @@ struct wm_case {
     double *d_modes = nullptr, *d_table = nullptr, *inflow_buf = nullptr;
     wm_inflow inflow{};
     long long inflow_n = 0;
-    bool sponge = false;
-    std::vector<double*> spmean;
-    int sponge_rows = 0;
-    double *d_cmf_part = nullptr, *d_dt_part = nullptr, *d_dt_tmp = nullptr, *d_cmf_delta = nullptr;
-    unsigned* d_counter = nullptr;       // [0]: CFL reduction, [1]: constant-mass-flux reduction
-    int dt_ctas = 0;
-    double Pr13 = 0, Pr3 = 0, kader_beta = 0;
-    // launch accounting / event timing (wm_profile_*)
-    long long nlaunch[WM_NKINDS] = {0, 0, 0, 0, 0};
-    bool prof = false;
-    struct Rec { int kind; cudaEvent_t a, b; };
-    std::vector<Rec> recs;
-    std::vector<cudaEvent_t> pool;
+    std::vector<double*> spmean;         // per block, null without sponge
+    View* self = nullptr;                // the case as a view of one case
+    Prof prof;
+    ~wm_case();
 };
 
 namespace {
 
-template <typename T>
-int dev_alloc(wm_case* c, T** p, size_t count) {
-    void* v = nullptr;
-    if (count == 0) count = 1;
-    cudaError_t e = cudaMalloc(&v, sizeof(T) * count);
-    if (e != cudaSuccess) return fail(WM_E_CUDA, "cudaMalloc(%zu bytes): %s", sizeof(T) * count, cudaGetErrorString(e));
-    c->allocs.push_back(v);
-    *p = static_cast<T*>(v);
-    return WM_OK;
-}
-
-template <typename T>
-int dev_upload(wm_case* c, T** p, const T* host, size_t count) {
-    int r = dev_alloc(c, p, count);
-    if (r) return r;
-    if (count && host) CK(cudaMemcpy(*p, host, sizeof(T) * count, cudaMemcpyHostToDevice));
-    return WM_OK;
-}
-
-cudaEvent_t pool_event(wm_case* c) {
-    if (!c->pool.empty()) {
-        cudaEvent_t e = c->pool.back();
-        c->pool.pop_back();
-        return e;
-    }
-    cudaEvent_t e = nullptr;
-    cudaEventCreate(&e);
-    return e;
-}
-
-// brackets one launch of `kind`: counts it and, when profiling, records an event pair
-struct LaunchScope {
-    wm_case* c;
-    int kind, slot = -1;
-    cudaStream_t s;
-    LaunchScope(wm_case* c_, int kind_, cudaStream_t s_, int n = 1) : c(c_), kind(kind_), s(s_) {
-        c->nlaunch[kind] += n;
-        if (c->prof) {
-            wm_case::Rec r{kind, pool_event(c), pool_event(c)};
-            cudaEventRecord(r.a, s);
-            c->recs.push_back(r);
-            slot = (int)c->recs.size() - 1;
-        }
-    }
-    ~LaunchScope() {
-        if (slot >= 0) cudaEventRecord(c->recs[slot].b, s);
-    }
+struct View {
+    Owner mem;
+    std::vector<wm_case*> members;
+    int nblocks = 0, ncases = 0;
+    std::vector<BlockDev> hb;
+    std::vector<CaseDev> hc;
+    std::vector<WallDev> hw;
+    std::vector<Tile> tiles;
+    std::vector<int> case_tile_start, case_block_start;
+    std::vector<GhostSeg> seg_rhs, seg_all;
+    int total_rhs = 0, total_all = 0;
+    BlockDev* d_blocks = nullptr;
+    CaseDev* d_cases = nullptr;
+    WallDev* d_walls = nullptr;
+    Tile* d_tiles = nullptr;
+    int* d_case_tile_start = nullptr;
+    GhostSeg *d_seg_rhs = nullptr, *d_seg_all = nullptr;
+    double *cmf_part = nullptr, *cmf_delta = nullptr, *dt_part = nullptr;
+    unsigned* counters = nullptr;        // [0]: CFL reduction, [1]: constant-mass-flux reduction
+    std::vector<int> cta_start;          // CFL pass: first CTA of each view block (+ total)
+    int max_wall_faces = 0, sponge_rows = 0;
+    bool any_sponge = false, any_cmf = false;
+    StageOpts opts{};
 };
 
 int upload_prog(wm_case* c, GhostProg* g, const wm_ghost_program& p) {
     g->count = p.count;
     int r;
-    if ((r = dev_upload(c, &g->dst, p.dst, 2 * (size_t)p.count))) return r;
-    if ((r = dev_upload(c, &g->src, p.src, 2 * (size_t)p.count))) return r;
-    if ((r = dev_upload(c, &g->ops, p.ops, 2 * (size_t)p.count))) return r;
-    if ((r = dev_upload(c, &g->op_code, p.op_code, (size_t)p.nops))) return r;
-    if ((r = dev_upload(c, &g->op_nrm, p.op_nrm, 3 * (size_t)p.nops))) return r;
+    if ((r = c->mem.upload(&g->dst, p.dst, 2 * (size_t)p.count))) return r;
+    if ((r = c->mem.upload(&g->src, p.src, 2 * (size_t)p.count))) return r;
+    if ((r = c->mem.upload(&g->ops, p.ops, 2 * (size_t)p.count))) return r;
+    if ((r = c->mem.upload(&g->op_code, p.op_code, (size_t)p.nops))) return r;
+    if ((r = c->mem.upload(&g->op_nrm, p.op_nrm, 3 * (size_t)p.nops))) return r;
     return WM_OK;
 }
 
@@ -178,25 +225,23 @@ int validate(const wm_case_desc* d) {
     return WM_OK;
 }
 
-int choose_chunk(wm_case* c, int tj, int tk, int requested) {
+// planes per stage-kernel CTA: wave quantisation against the chunk prologue cost
+int choose_chunk(const std::vector<BlockDev>& hb, const StageOpts& opts, int tj, int tk, int requested) {
     if (requested > 0) return requested;
     int sms = 148, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int occ = stage_ctas_per_sm(c->opts);
+    int occ = stage_ctas_per_sm(opts);
     if (occ < 1) occ = 1;
     const long long slots = (long long)sms * occ;
     int nimax = 0;
-    long long jk = 0;
-    for (const BlockDev& B : c->hb) {
-        nimax = std::max(nimax, B.n[0]);
-    }
+    for (const BlockDev& B : hb) nimax = std::max(nimax, B.n[0]);
     double best = 1e300;
     int best_ic = nimax;
     for (int ic = 4; ic <= std::max(4, nimax); ++ic) {
         long long ctas = 0;
-        for (const BlockDev& B : c->hb) {
-            jk = (long long)((B.n[1] + tj - 1) / tj) * ((B.n[2] + tk - 1) / tk);
+        for (const BlockDev& B : hb) {
+            const long long jk = (long long)((B.n[1] + tj - 1) / tj) * ((B.n[2] + tk - 1) / tk);
             ctas += jk * ((B.n[0] + ic - 1) / ic);
         }
         const long long waves = (ctas + slots - 1) / slots;
@@ -208,7 +253,7 @@ int choose_chunk(wm_case* c, int tj, int tk, int requested) {
 
 void build_tiles(wm_case* c, int tj, int tk, int ic) {
     c->tiles.clear();
-    for (int b = 0; b < c->nblocks; ++b) {
+    for (int b = 0; b < (int)c->hb.size(); ++b) {
         const BlockDev& B = c->hb[b];
         const int ng = B.ng;
         for (int i0 = ng; i0 < ng + B.n[0]; i0 += ic)
@@ -218,106 +263,208 @@ void build_tiles(wm_case* c, int tj, int tk, int ic) {
     }
 }
 
-GhostArgs ghost_args(wm_case* c, const GhostProg& g, double* const* q, bool two_phase) {
-    GhostArgs G{};
-    G.count = g.count;
-    G.dst = g.dst; G.src = g.src; G.ops = g.ops; G.op_code = g.op_code; G.op_nrm = g.op_nrm;
-    G.bc = c->d_bc;
-    G.inflow = c->inflow_buf;
-    G.inflow_n = c->inflow_n;
-    G.stash = two_phase ? c->stash : nullptr;
-    G.gamma = c->hc.gamma; G.gm1 = c->hc.gm1; G.Rg = c->hc.Rg;
-    for (int b = 0; b < c->nblocks; ++b) { G.q[b] = q[b]; G.ncell[b] = c->hb[b].ncell; }
-    return G;
+bool same_opts(const StageOpts& a, const StageOpts& b) {
+    return a.precision == b.precision && a.scheme == b.scheme && a.kep_order == b.kep_order &&
+           a.limiter == b.limiter && a.sgs == b.sgs && a.tile == b.tile;
 }
 
-int fill_inflow(wm_case* c, double time0, double time_dt, const double* dt, cudaStream_t s) {
-    if (!c->has_inflow) return WM_OK;
-    const BlockDev& B = c->hb[c->inflow_block];
-    InflowArgs I{};
-    I.block = c->d_blocks + c->inflow_block;
-    I.modes = c->d_modes; I.table = c->d_table;
-    I.n_modes = c->inflow.n_modes; I.n_tab = c->inflow.n_tab;
-    I.U_inf = c->inflow.U_inf; I.L = c->inflow.L; I.rho_inf = c->inflow.rho_inf; I.p_inf = c->inflow.p_inf;
-    I.gm1 = c->hc.gm1;
-    I.time0 = time0; I.time_dt = time_dt; I.dt = dt;
-    I.out = c->inflow_buf;
-    LaunchScope ls(c, WM_KIND_SOURCE, s);
-    CK(launch_inflow(I, B.N[1], B.N[2], B.ng, s));
+GhostSeg segment(const wm_case* c, const GhostProg& p, int start, int block0) {
+    GhostSeg g{};
+    g.dst = p.dst; g.src = p.src; g.ops = p.ops; g.op_code = p.op_code; g.op_nrm = p.op_nrm;
+    g.bc = c->d_bc;
+    g.inflow = c->inflow_buf;
+    g.inflow_n = c->inflow_n;
+    g.start = start; g.count = p.count; g.block0 = block0;
+    g.gamma = c->hc.gamma; g.gm1 = c->hc.gm1; g.Rg = c->hc.Rg;
+    return g;
+}
+
+// concatenated device tables and reduction scratch of `cases`
+int build_view(View* v, wm_case* const* cases, int n) {
+    if (n < 1 || n > MAX_CASES) return fail(WM_E_INVALID, "a view holds 1..%d cases, got %d", MAX_CASES, n);
+    for (int ci = 0; ci < n; ++ci) {
+        wm_case* c = cases[ci];
+        if (!c) return fail(WM_E_INVALID, "null case %d", ci);
+        if (ci > 0 && !same_opts(c->opts, cases[0]->opts))
+            return fail(WM_E_UNSUPPORTED, "cases of one batch must share precision, scheme, SGS model and tile shape");
+        const int bo = (int)v->hb.size(), wo = (int)v->hw.size();
+        if (bo + (int)c->hb.size() > WM_MAX_BLOCKS)
+            return fail(WM_E_UNSUPPORTED, "a batch holds at most %d blocks", WM_MAX_BLOCKS);
+        v->members.push_back(c);
+        v->case_block_start.push_back(bo);
+        v->case_tile_start.push_back((int)v->tiles.size());
+        for (BlockDev B : c->hb) {
+            B.case_id = ci;
+            for (int f = 0; f < 6; ++f)
+                if (B.wall[f] >= 0) B.wall[f] += wo;
+            v->hb.push_back(B);
+        }
+        for (WallDev W : c->hw) {
+            W.block += bo;
+            v->max_wall_faces = std::max(v->max_wall_faces, W.nt1 * W.nt2);
+            v->hw.push_back(W);
+        }
+        v->hc.push_back(c->hc);
+        for (Tile t : c->tiles) {
+            t.blk += bo;
+            v->tiles.push_back(t);
+        }
+        v->seg_rhs.push_back(segment(c, c->prog_rhs, v->total_rhs, bo));
+        v->total_rhs += c->prog_rhs.count;
+        v->seg_all.push_back(segment(c, c->prog_all, v->total_all, bo));
+        v->total_all += c->prog_all.count;
+        for (size_t b = 0; b < c->hb.size(); ++b)
+            if (c->spmean[b]) v->sponge_rows = std::max(v->sponge_rows, c->hb[b].n[0] * c->hb[b].n[1]);
+        v->any_sponge = v->any_sponge || c->hc.sponge;
+        v->any_cmf = v->any_cmf || c->hc.cmf_dir >= 0;
+    }
+    v->case_block_start.push_back((int)v->hb.size());
+    v->case_tile_start.push_back((int)v->tiles.size());
+    v->nblocks = (int)v->hb.size();
+    v->ncases = n;
+    v->opts = cases[0]->opts;
+    v->cta_start.assign(1, 0);                  // one interior cell per thread of the CFL pass
+    for (const BlockDev& B : v->hb)
+        v->cta_start.push_back(v->cta_start.back() + (int)(((long long)B.n[0] * B.n[1] * B.n[2] + DT_NT - 1) / DT_NT));
+    int r;
+    Owner& m = v->mem;
+    if ((r = m.upload(&v->d_blocks, v->hb.data(), v->hb.size()))) return r;
+    if ((r = m.upload(&v->d_cases, v->hc.data(), v->hc.size()))) return r;
+    if ((r = m.upload(&v->d_walls, v->hw.data(), v->hw.size()))) return r;
+    if ((r = m.upload(&v->d_tiles, v->tiles.data(), v->tiles.size()))) return r;
+    if ((r = m.upload(&v->d_case_tile_start, v->case_tile_start.data(), v->case_tile_start.size()))) return r;
+    if ((r = m.upload(&v->d_seg_rhs, v->seg_rhs.data(), v->seg_rhs.size()))) return r;
+    if ((r = m.upload(&v->d_seg_all, v->seg_all.data(), v->seg_all.size()))) return r;
+    if ((r = m.alloc(&v->cmf_part, v->tiles.size()))) return r;
+    if ((r = m.alloc(&v->cmf_delta, (size_t)n))) return r;
+    CK(cudaMemset(v->cmf_delta, 0, sizeof(double) * n));
+    if ((r = m.alloc(&v->dt_part, (size_t)v->cta_start.back()))) return r;
+    if ((r = m.alloc(&v->counters, 2))) return r;
+    CK(cudaMemset(v->counters, 0, 2 * sizeof(unsigned)));
     return WM_OK;
 }
 
-// one RHS evaluation fused with RK stage `stage` (0 = plain RHS)
-int run_stage(wm_case* c, int stage, double* const* q_in, const double* const* q0, double* const* q_out,
-              const double* dt, double time0, double time_dt, cudaStream_t s) {
-    int r;
-    if ((r = fill_inflow(c, time0, time_dt, dt, s))) return r;
-    {
-        LaunchScope ls(c, WM_KIND_GHOST, s, c->prog_rhs.count ? 1 : 0);
-        CK(launch_ghost(ghost_args(c, c->prog_rhs, q_in, false), s));
+int fill_inflow(View* v, Prof* pf, const double* times, double time_dt, const double* const* dt, cudaStream_t s) {
+    for (int ci = 0; ci < v->ncases; ++ci) {
+        wm_case* c = v->members[ci];
+        if (!c->has_inflow) continue;
+        const int vb = v->case_block_start[ci] + c->inflow_block;
+        const BlockDev& B = v->hb[vb];
+        InflowArgs I{};
+        I.block = v->d_blocks + vb;
+        I.modes = c->d_modes; I.table = c->d_table;
+        I.n_modes = c->inflow.n_modes; I.n_tab = c->inflow.n_tab;
+        I.U_inf = c->inflow.U_inf; I.L = c->inflow.L; I.rho_inf = c->inflow.rho_inf; I.p_inf = c->inflow.p_inf;
+        I.gm1 = c->hc.gm1;
+        I.time0 = times[ci]; I.time_dt = time_dt; I.dt = dt ? dt[ci] : nullptr;
+        I.out = c->inflow_buf;
+        LaunchScope ls(pf, WM_KIND_SOURCE, s);
+        CK(launch_inflow(I, B.N[1], B.N[2], B.ng, s));
     }
-    if (!c->hw.empty()) {
+    return WM_OK;
+}
+
+// one RHS evaluation fused with RK stage `stage` (0 = plain RHS) for every case of the view;
+// state pointers per view block, time steps and times per case
+int run_stage(View* v, Prof* pf, int stage, double* const* q_in, const double* const* q0, double* const* q_out,
+              const double* const* dt, const double* times, double time_dt, cudaStream_t s) {
+    int r;
+    if ((r = fill_inflow(v, pf, times, time_dt, dt, s))) return r;
+    {
+        GhostArgs G{};
+        G.segs = v->d_seg_rhs; G.nseg = v->ncases; G.total = v->total_rhs; G.stash = nullptr;
+        for (int b = 0; b < v->nblocks; ++b) { G.q[b] = q_in[b]; G.ncell[b] = v->hb[b].ncell; }
+        LaunchScope ls(pf, WM_KIND_GHOST, s, G.total ? 1 : 0);
+        CK(launch_ghost(G, s));
+    }
+    if (!v->hw.empty()) {
         WallArgs W{};
-        W.blocks = c->d_blocks; W.cases = c->d_case; W.walls = c->d_walls;
-        W.nwalls = (int)c->hw.size(); W.max_faces = c->max_wall_faces;
-        W.Pr13 = c->Pr13; W.Pr3 = c->Pr3; W.kader_beta = c->kader_beta;
-        for (int b = 0; b < c->nblocks; ++b) W.q[b] = q_in[b];
-        LaunchScope ls(c, WM_KIND_WALL, s);
+        W.blocks = v->d_blocks; W.cases = v->d_cases; W.walls = v->d_walls;
+        W.nwalls = (int)v->hw.size(); W.max_faces = v->max_wall_faces;
+        for (int b = 0; b < v->nblocks; ++b) W.q[b] = q_in[b];
+        LaunchScope ls(pf, WM_KIND_WALL, s);
         CK(launch_wall(W, s));
     }
-    if (c->sponge) {
+    std::vector<const double*> spm(v->nblocks, nullptr);
+    if (v->any_sponge) {
         SpongeArgs S{};
-        S.blocks = c->d_blocks; S.nblocks = c->nblocks;
-        for (int b = 0; b < c->nblocks; ++b) { S.q[b] = q_in[b]; S.mean[b] = c->spmean[b]; }
-        LaunchScope ls(c, WM_KIND_SOURCE, s);
-        CK(launch_sponge_mean(S, c->sponge_rows, s));
+        S.blocks = v->d_blocks; S.nblocks = v->nblocks;
+        for (int ci = 0; ci < v->ncases; ++ci)
+            for (size_t b = 0; b < v->members[ci]->hb.size(); ++b) {
+                const int vb = v->case_block_start[ci] + (int)b;
+                S.q[vb] = q_in[vb];
+                S.mean[vb] = v->members[ci]->spmean[b];
+                spm[vb] = S.mean[vb];
+            }
+        LaunchScope ls(pf, WM_KIND_SOURCE, s);
+        CK(launch_sponge_mean(S, v->sponge_rows, s));
     }
     StageArgs A{};
-    A.blocks = c->d_blocks; A.cases = c->d_case; A.walls = c->d_walls;
-    A.tiles = c->d_tiles; A.ntiles = (int)c->tiles.size();
-    A.stage = stage; A.dt = dt;
-    A.cmf_part = (stage == 3 && c->hc.cmf_dir >= 0) ? c->d_cmf_part : nullptr;
-    A.cmf_counter = c->d_counter + 1;
-    A.cmf_delta = c->d_cmf_delta;
-    for (int b = 0; b < c->nblocks; ++b) {
+    A.blocks = v->d_blocks; A.cases = v->d_cases; A.walls = v->d_walls;
+    A.tiles = v->d_tiles; A.ntiles = (int)v->tiles.size();
+    A.stage = stage;
+    A.ncases = v->ncases;
+    A.case_tile_start = v->d_case_tile_start;
+    A.cmf_part = (stage == 3 && v->any_cmf) ? v->cmf_part : nullptr;
+    A.cmf_counter = v->counters + 1;
+    A.cmf_delta = v->cmf_delta;
+    for (int ci = 0; ci < v->ncases; ++ci) A.dt[ci] = dt ? dt[ci] : nullptr;
+    for (int b = 0; b < v->nblocks; ++b) {
         A.p[b].q_in = q_in[b];
         A.p[b].q0 = q0 ? q0[b] : q_in[b];
         A.p[b].q_out = q_out[b];
-        A.p[b].spmean = c->sponge ? c->spmean[b] : nullptr;
+        A.p[b].spmean = spm[b];
     }
-    LaunchScope ls(c, WM_KIND_STAGE, s);
-    CK(launch_stage(A, c->opts, s));
+    LaunchScope ls(pf, WM_KIND_STAGE, s);
+    CK(launch_stage(A, v->opts, s));
     return WM_OK;
 }
 
-int run_dt(wm_case* c, double* const* q, bool apply_cmf, bool want_dt, double* dt_out, cudaStream_t s) {
+int run_dt(View* v, Prof* pf, double* const* q, bool apply_cmf, bool want_dt, double* const* dt_out, cudaStream_t s) {
     DtArgs D{};
-    D.blocks = c->d_blocks; D.cases = c->d_case; D.nblocks = c->nblocks;
-    D.ctas_per_block = c->dt_ctas;
-    for (int b = 0; b < c->nblocks; ++b) D.q[b] = q[b];
-    D.cmf_delta = apply_cmf ? c->d_cmf_delta : nullptr;
+    D.blocks = v->d_blocks; D.cases = v->d_cases; D.nblocks = v->nblocks;
+    D.ncta = v->cta_start.back();
+    for (int b = 0; b <= v->nblocks; ++b) D.cta_start[b] = v->cta_start[b];
+    D.ncases = v->ncases;
+    for (int ci = 0; ci <= v->ncases; ++ci) D.case_block_start[ci] = v->case_block_start[ci];
+    for (int b = 0; b < v->nblocks; ++b) D.q[b] = q[b];
+    D.cmf_delta = apply_cmf ? v->cmf_delta : nullptr;
     D.want_dt = want_dt ? 1 : 0;
-    D.dt_part = c->d_dt_part; D.counter = c->d_counter;
-    D.dt_out = dt_out ? dt_out : c->d_dt_tmp;
-    LaunchScope ls(c, WM_KIND_DT, s);
+    D.dt_part = v->dt_part; D.counter = v->counters;
+    for (int ci = 0; ci < v->ncases; ++ci) D.dt_out[ci] = dt_out ? dt_out[ci] : nullptr;
+    LaunchScope ls(pf, WM_KIND_DT, s);
     CK(launch_dt(D, s));
     return WM_OK;
 }
 
+// SSP-RK3 of every case of the view with work states w0/w1 (per view block), then the
+// constraint pass; with want_next the pass also writes each case's next CFL time step
+int run_step(View* v, Prof* pf, double* const* q_in, double* const* q_out, double* const* w0, double* const* w1,
+             const double* const* dt, double* const* dt_next, const double* times, bool want_next, cudaStream_t s) {
+    int r;
+    if ((r = run_stage(v, pf, 1, q_in, q_in, w0, dt, times, 0.0, s))) return r;
+    if ((r = run_stage(v, pf, 2, w0, q_in, w1, dt, times, 1.0, s))) return r;
+    if ((r = run_stage(v, pf, 3, w1, q_in, q_out, dt, times, 0.5, s))) return r;
+    if (want_next || v->any_cmf) return run_dt(v, pf, q_out, v->any_cmf, want_next, dt_next, s);
+    return WM_OK;
+}
+
 }  // namespace
+
+wm_case::~wm_case() { delete self; }
+
+struct wm_batch {
+    View view;
+    Prof prof;
+    std::vector<double*> w0, w1;     // per view block: the member cases' work states
+};
 
 extern "C" {
 
 int wm_version(void) { return WM_ABI_VERSION; }
 const char* wm_last_error(void) { return g_err.c_str(); }
 
-void wm_case_destroy(wm_case* c) {
-    if (!c) return;
-    for (auto& r : c->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
-    for (cudaEvent_t e : c->pool) cudaEventDestroy(e);
-    for (void* p : c->allocs) cudaFree(p);
-    delete c;
-}
+void wm_case_destroy(wm_case* c) { delete c; }
 
 int wm_case_create(const wm_case_desc* d, wm_case** out) {
     if (!out) return fail(WM_E_INVALID, "null output handle");
@@ -325,9 +472,8 @@ int wm_case_create(const wm_case_desc* d, wm_case** out) {
     int r = validate(d);
     if (r) return r;
     wm_case* c = new wm_case();
-    auto bail = [&](int code) { wm_case_destroy(c); return code; };
+    auto bail = [&](int code) { delete c; return code; };
     CK(cudaGetDevice(&c->device));
-    c->nblocks = d->nblocks;
 
     // ---- physical constants
     const wm_gas& g = d->gas;
@@ -342,6 +488,9 @@ int wm_case_create(const wm_case_desc* d, wm_case** out) {
     C.sgs_c = d->sgs_coeff;
     C.cfl = d->cfl;
     C.nu_fac = std::max(4.0 / 3.0, g.gamma / g.Pr);
+    C.Pr13 = std::pow(g.Pr, 1.0 / 3.0);
+    C.Pr3 = std::pow(g.Pr, 3.0);
+    C.kader_beta = std::pow(3.85 * std::pow(g.Pr, 1.0 / 3.0) - 1.3, 2.0) + 2.12 * std::log(g.Pr);
     C.cmf_dir = d->cmf_dir; C.cmf_target = d->cmf_target; C.cmf_volume = d->cmf_volume;
     C.sponge = d->sponge.enabled;
     if (C.sponge) {
@@ -350,9 +499,6 @@ int wm_case_create(const wm_case_desc* d, wm_case** out) {
         C.sp_sigma0 = d->sponge.strength * d->sponge.U_inf / d->sponge.L;
         C.sp_invL = 1.0 / d->sponge.L;
     }
-    c->Pr13 = std::pow(g.Pr, 1.0 / 3.0);
-    c->Pr3 = std::pow(g.Pr, 3.0);
-    c->kader_beta = std::pow(3.85 * std::pow(g.Pr, 1.0 / 3.0) - 1.3, 2.0) + 2.12 * std::log(g.Pr);
     c->opts = StageOpts{d->precision, d->scheme, d->kep_order, d->limiter, d->sgs, d->tile < 0 ? 0 : d->tile};
 
     // ---- blocks, metrics, work buffers
@@ -370,19 +516,19 @@ int wm_case_create(const wm_case_desc* d, wm_case** out) {
             return bail(fail(WM_E_UNSUPPORTED, "block %d: %lld cells exceed the 32-bit metric index range "
                              "(split the block)", b, B.ncell));
         double* met = nullptr;
-        if ((r = dev_upload(c, &met, src.metrics, (size_t)WM_NMET * B.ncell))) return bail(r);
+        if ((r = c->mem.upload(&met, src.metrics, (size_t)WM_NMET * B.ncell))) return bail(r);
         B.met = met;
         B.met32 = nullptr;
         if (d->precision == WM_PREC_MIXED) {
             std::vector<float> m32((size_t)WM_NMET * B.ncell);
             for (size_t i = 0; i < m32.size(); ++i) m32[i] = (float)src.metrics[i];
             float* p32 = nullptr;
-            if ((r = dev_upload(c, &p32, m32.data(), m32.size()))) return bail(r);
+            if ((r = c->mem.upload(&p32, m32.data(), m32.size()))) return bail(r);
             B.met32 = p32;
         }
         for (int s = 0; s < 2; ++s) {
             double* w = nullptr;
-            if ((r = dev_alloc(c, &w, 5 * (size_t)B.ncell))) return bail(r);
+            if ((r = c->mem.alloc(&w, 5 * (size_t)B.ncell))) return bail(r);
             CK(cudaMemset(w, 0, sizeof(double) * 5 * B.ncell));
             c->work[s].push_back(w);
         }
@@ -400,22 +546,20 @@ int wm_case_create(const wm_case_desc* d, wm_case** out) {
         W.T_wall = src.T_wall; W.kappa = src.kappa; W.B = src.B; W.ekb = std::exp(-src.kappa * src.B);
         const size_t nf = (size_t)W.nt1 * W.nt2;
         double* gm = nullptr;
-        if ((r = dev_upload(c, &gm, src.geom, 5 * nf))) return bail(r);
+        if ((r = c->mem.upload(&gm, src.geom, 5 * nf))) return bail(r);
         W.geom = gm;
-        if ((r = dev_alloc(c, &W.F, 5 * nf))) return bail(r);
-        if ((r = dev_alloc(c, &W.tq, 2 * nf))) return bail(r);
-        c->max_wall_faces = std::max(c->max_wall_faces, (int)nf);
+        if ((r = c->mem.alloc(&W.F, 5 * nf))) return bail(r);
+        if ((r = c->mem.alloc(&W.tq, 2 * nf))) return bail(r);
         if (B.wall[2 * src.axis + src.side] >= 0) return bail(fail(WM_E_INVALID, "two walls on one face"));
         B.wall[2 * src.axis + src.side] = w;
         c->hw.push_back(W);
     }
-    if ((r = dev_upload(c, &c->d_walls, c->hw.data(), c->hw.size()))) return bail(r);
 
     // ---- ghost programs and BC constants
-    if ((r = dev_upload(c, &c->d_bc, d->bc_table, 8 * (size_t)std::max(d->nbc, 1)))) return bail(r);
+    if ((r = c->mem.upload(&c->d_bc, d->bc_table, 8 * (size_t)std::max(d->nbc, 1)))) return bail(r);
     if ((r = upload_prog(c, &c->prog_rhs, d->ghost_rhs))) return bail(r);
     if ((r = upload_prog(c, &c->prog_all, d->ghost_all))) return bail(r);
-    if ((r = dev_alloc(c, &c->stash, 5 * (size_t)std::max(d->ghost_all.count, 1)))) return bail(r);
+    if ((r = c->mem.alloc(&c->stash, 5 * (size_t)std::max(d->ghost_all.count, 1)))) return bail(r);
 
     // ---- synthetic inflow
     if (d->inflow) {
@@ -424,46 +568,30 @@ int wm_case_create(const wm_case_desc* d, wm_case** out) {
         c->has_inflow = true;
         c->inflow = I;
         c->inflow_block = I.block;
-        if ((r = dev_upload(c, &c->d_modes, I.modes, 12 * (size_t)I.n_modes))) return bail(r);
-        if ((r = dev_upload(c, &c->d_table, I.table, 7 * (size_t)I.n_tab))) return bail(r);
+        if ((r = c->mem.upload(&c->d_modes, I.modes, 12 * (size_t)I.n_modes))) return bail(r);
+        if ((r = c->mem.upload(&c->d_table, I.table, 7 * (size_t)I.n_tab))) return bail(r);
         const BlockDev& B = c->hb[I.block];
         c->inflow_n = (long long)B.ng * B.plane;
-        if ((r = dev_alloc(c, &c->inflow_buf, 5 * (size_t)c->inflow_n))) return bail(r);
+        if ((r = c->mem.alloc(&c->inflow_buf, 5 * (size_t)c->inflow_n))) return bail(r);
     }
 
     // ---- sponge means
+    c->spmean.assign(d->nblocks, nullptr);
     if (d->sponge.enabled) {
-        c->sponge = true;
         for (int b = 0; b < d->nblocks; ++b) {
             const BlockDev& B = c->hb[b];
-            double* m = nullptr;
-            if ((r = dev_alloc(c, &m, 5 * (size_t)B.N[0] * B.N[1]))) return bail(r);
-            c->spmean.push_back(m);
-            c->sponge_rows = std::max(c->sponge_rows, B.n[0] * B.n[1]);
+            if ((r = c->mem.alloc(&c->spmean[b], 5 * (size_t)B.N[0] * B.N[1]))) return bail(r);
         }
     }
 
-    // ---- tiles, reduction scratch
+    // ---- stage tiles (fixed per case: results do not depend on batch membership)
     int tj, tk;
     tile_shape(c->opts.tile, &tj, &tk);
-    build_tiles(c, tj, tk, choose_chunk(c, tj, tk, d->chunk));
-    if ((r = dev_upload(c, &c->d_tiles, c->tiles.data(), c->tiles.size()))) return bail(r);
-    if ((r = dev_alloc(c, &c->d_cmf_part, c->tiles.size()))) return bail(r);
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-    long long maxcells = 0;
-    for (const BlockDev& B : c->hb) maxcells = std::max(maxcells, (long long)B.n[0] * B.n[1] * B.n[2]);
-    (void)sms;
-    c->dt_ctas = (int)std::max(1LL, (maxcells + 255) / 256);      // one interior cell per thread
-    if ((r = dev_alloc(c, &c->d_dt_part, (size_t)c->dt_ctas * d->nblocks))) return bail(r);
-    if ((r = dev_alloc(c, &c->d_counter, 2))) return bail(r);
-    CK(cudaMemset(c->d_counter, 0, 2 * sizeof(unsigned)));
-    if ((r = dev_alloc(c, &c->d_cmf_delta, 1))) return bail(r);
-    CK(cudaMemset(c->d_cmf_delta, 0, sizeof(double)));
-    if ((r = dev_alloc(c, &c->d_dt_tmp, 1))) return bail(r);
+    build_tiles(c, tj, tk, choose_chunk(c->hb, c->opts, tj, tk, d->chunk));
 
-    if ((r = dev_upload(c, &c->d_case, &c->hc, 1))) return bail(r);
-    if ((r = dev_upload(c, &c->d_blocks, c->hb.data(), c->hb.size()))) return bail(r);
+    c->self = new View();
+    wm_case* self_list[1] = {c};
+    if ((r = build_view(c->self, self_list, 1))) return bail(r);
     CK(cudaDeviceSynchronize());
     *out = c;
     return WM_OK;
@@ -472,35 +600,32 @@ int wm_case_create(const wm_case_desc* d, wm_case** out) {
 int wm_apply_bcs(wm_case* c, double* const* q, double time, void* stream) {
     if (!c || !q) return fail(WM_E_INVALID, "null argument");
     cudaStream_t s = (cudaStream_t)stream;
+    View* v = c->self;
     int r;
-    if ((r = fill_inflow(c, time, 0.0, nullptr, s))) return r;
-    LaunchScope ls(c, WM_KIND_GHOST, s, c->prog_all.count ? 2 : 0);
-    CK(launch_ghost(ghost_args(c, c->prog_all, q, true), s));
+    if ((r = fill_inflow(v, &c->prof, &time, 0.0, nullptr, s))) return r;
+    GhostArgs G{};
+    G.segs = v->d_seg_all; G.nseg = 1; G.total = v->total_all; G.stash = c->stash;
+    for (int b = 0; b < v->nblocks; ++b) { G.q[b] = q[b]; G.ncell[b] = v->hb[b].ncell; }
+    LaunchScope ls(&c->prof, WM_KIND_GHOST, s, G.total ? 2 : 0);
+    CK(launch_ghost(G, s));
     return WM_OK;
 }
 
 int wm_rhs(wm_case* c, double* const* q, double* const* rr, double time, void* stream) {
     if (!c || !q || !rr) return fail(WM_E_INVALID, "null argument");
-    return run_stage(c, 0, q, nullptr, rr, nullptr, time, 0.0, (cudaStream_t)stream);
+    return run_stage(c->self, &c->prof, 0, q, nullptr, rr, nullptr, &time, 0.0, (cudaStream_t)stream);
 }
 
 int wm_max_dt(wm_case* c, const double* const* q, double* dt_dev, void* stream) {
     if (!c || !q || !dt_dev) return fail(WM_E_INVALID, "null argument");
-    return run_dt(c, const_cast<double* const*>(q), false, true, dt_dev, (cudaStream_t)stream);
+    return run_dt(c->self, &c->prof, const_cast<double* const*>(q), false, true, &dt_dev, (cudaStream_t)stream);
 }
 
 int wm_advance(wm_case* c, double* const* q_in, double* const* q_out, const double* dt_dev, double time,
                void* stream) {
     if (!c || !q_in || !q_out || !dt_dev) return fail(WM_E_INVALID, "null argument");
-    cudaStream_t s = (cudaStream_t)stream;
-    int r;
-    double* const* w0 = c->work[0].data();
-    double* const* w1 = c->work[1].data();
-    if ((r = run_stage(c, 1, q_in, q_in, w0, dt_dev, time, 0.0, s))) return r;
-    if ((r = run_stage(c, 2, w0, q_in, w1, dt_dev, time, 1.0, s))) return r;
-    if ((r = run_stage(c, 3, w1, q_in, q_out, dt_dev, time, 0.5, s))) return r;
-    if (c->hc.cmf_dir >= 0 && (r = run_dt(c, q_out, true, false, nullptr, s))) return r;
-    return WM_OK;
+    return run_step(c->self, &c->prof, q_in, q_out, c->work[0].data(), c->work[1].data(), &dt_dev, nullptr, &time,
+                    false, (cudaStream_t)stream);
 }
 
 int wm_step(wm_case* c, double* const* q_in, double* const* q_out, double* dt_dev, double time, void* stream) {
@@ -512,49 +637,76 @@ int wm_step(wm_case* c, double* const* q_in, double* const* q_out, double* dt_de
 int wm_step_fused(wm_case* c, double* const* q_in, double* const* q_out, const double* dt_in, double* dt_next,
                   double time, void* stream) {
     if (!c || !q_in || !q_out || !dt_in || !dt_next) return fail(WM_E_INVALID, "null argument");
-    cudaStream_t s = (cudaStream_t)stream;
-    int r;
-    double* const* w0 = c->work[0].data();
-    double* const* w1 = c->work[1].data();
-    if ((r = run_stage(c, 1, q_in, q_in, w0, dt_in, time, 0.0, s))) return r;
-    if ((r = run_stage(c, 2, w0, q_in, w1, dt_in, time, 1.0, s))) return r;
-    if ((r = run_stage(c, 3, w1, q_in, q_out, dt_in, time, 0.5, s))) return r;
-    return run_dt(c, q_out, c->hc.cmf_dir >= 0, true, dt_next, s);
+    return run_step(c->self, &c->prof, q_in, q_out, c->work[0].data(), c->work[1].data(), &dt_in, &dt_next, &time,
+                    true, (cudaStream_t)stream);
 }
 
 int wm_wall_stats(wm_case* c, const double* const* q, double* const* out, void* stream) {
     if (!c || !q || !out) return fail(WM_E_INVALID, "null argument");
     cudaStream_t s = (cudaStream_t)stream;
-    if (c->hw.empty()) return WM_OK;
+    View* v = c->self;
+    if (v->hw.empty()) return WM_OK;
     WallArgs W{};
-    W.blocks = c->d_blocks; W.cases = c->d_case; W.walls = c->d_walls;
-    W.nwalls = (int)c->hw.size(); W.max_faces = c->max_wall_faces;
-    W.Pr13 = c->Pr13; W.Pr3 = c->Pr3; W.kader_beta = c->kader_beta;
-    for (int b = 0; b < c->nblocks; ++b) W.q[b] = q[b];
+    W.blocks = v->d_blocks; W.cases = v->d_cases; W.walls = v->d_walls;
+    W.nwalls = (int)v->hw.size(); W.max_faces = v->max_wall_faces;
+    for (int b = 0; b < v->nblocks; ++b) W.q[b] = q[b];
     {
-        LaunchScope ls(c, WM_KIND_WALL, s);
+        LaunchScope ls(&c->prof, WM_KIND_WALL, s);
         CK(launch_wall(W, s));
     }
-    for (size_t w = 0; w < c->hw.size(); ++w) {
-        const size_t nf = (size_t)c->hw[w].nt1 * c->hw[w].nt2;
-        CK(cudaMemcpyAsync(out[w], c->hw[w].tq, sizeof(double) * 2 * nf, cudaMemcpyDeviceToDevice, s));
+    for (size_t w = 0; w < v->hw.size(); ++w) {
+        const size_t nf = (size_t)v->hw[w].nt1 * v->hw[w].nt2;
+        CK(cudaMemcpyAsync(out[w], v->hw[w].tq, sizeof(double) * 2 * nf, cudaMemcpyDeviceToDevice, s));
     }
+    return WM_OK;
+}
+
+int wm_batch_create(int ncases, wm_case* const* cases, wm_batch** out) {
+    if (!out || !cases) return fail(WM_E_INVALID, "null argument");
+    *out = nullptr;
+    wm_batch* b = new wm_batch();
+    int r = build_view(&b->view, cases, ncases);
+    if (r) { delete b; return r; }
+    for (int ci = 0; ci < ncases; ++ci)
+        for (size_t k = 0; k < cases[ci]->hb.size(); ++k) {
+            b->w0.push_back(cases[ci]->work[0][k]);
+            b->w1.push_back(cases[ci]->work[1][k]);
+        }
+    *out = b;
+    return WM_OK;
+}
+
+void wm_batch_destroy(wm_batch* b) { delete b; }
+
+int wm_batch_step(wm_batch* b, double* const* q_in, double* const* q_out, const double* const* dt_in,
+                  double* const* dt_next, const double* times, void* stream) {
+    if (!b || !q_in || !q_out || !dt_in || !dt_next || !times) return fail(WM_E_INVALID, "null argument");
+    return run_step(&b->view, &b->prof, q_in, q_out, b->w0.data(), b->w1.data(), dt_in, dt_next, times, true,
+                    (cudaStream_t)stream);
+}
+
+int wm_batch_info(wm_batch* b, int* nblocks, int* ntiles, long long* launches_per_step) {
+    if (!b) return fail(WM_E_INVALID, "null batch");
+    const View& v = b->view;
+    int inflow = 0;
+    for (wm_case* c : v.members) inflow += c->has_inflow ? 1 : 0;
+    const long long per_stage = inflow + (v.total_rhs ? 1 : 0) + (v.hw.empty() ? 0 : 1) + (v.any_sponge ? 1 : 0) + 1;
+    if (nblocks) *nblocks = v.nblocks;
+    if (ntiles) *ntiles = (int)v.tiles.size();
+    if (launches_per_step) *launches_per_step = 3 * per_stage + 1;
     return WM_OK;
 }
 
 int wm_profile_enable(wm_case* c, int enable) {
     if (!c) return fail(WM_E_INVALID, "null case");
-    for (auto& r : c->recs) { c->pool.push_back(r.a); c->pool.push_back(r.b); }
-    c->recs.clear();
-    for (int k = 0; k < WM_NKINDS; ++k) c->nlaunch[k] = 0;
-    c->prof = enable != 0;
+    c->prof.reset(enable != 0);
     return WM_OK;
 }
 
 int wm_profile_read(wm_case* c, int kind, double* ms_total, long long* launches) {
     if (!c || kind < -1 || kind >= WM_NKINDS) return fail(WM_E_INVALID, "bad profile query");
     double ms = 0.0;
-    for (auto& r : c->recs) {
+    for (auto& r : c->prof.recs) {
         if (kind >= 0 && r.kind != kind) continue;
         CK(cudaEventSynchronize(r.b));
         float t = 0.f;
@@ -563,7 +715,7 @@ int wm_profile_read(wm_case* c, int kind, double* ms_total, long long* launches)
     }
     long long n = 0;
     for (int k = 0; k < WM_NKINDS; ++k)
-        if (kind < 0 || k == kind) n += c->nlaunch[k];
+        if (kind < 0 || k == kind) n += c->prof.nlaunch[k];
     if (ms_total) *ms_total = ms;
     if (launches) *launches = n;
     return WM_OK;

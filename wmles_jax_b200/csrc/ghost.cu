@@ -89,41 +89,53 @@ __device__ __forceinline__ void op_farfield(double q[5], const double nrm[3], in
     g_p2c(o, gm1, q);
 }
 
+// segment (case) holding launch entry e: segments are in entry order
+__device__ __forceinline__ int find_seg(const GhostArgs& G, int e) {
+    int lo = 0, hi = G.nseg - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (G.segs[mid].start <= e) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
 __global__ void ghost_gather_kernel(const __grid_constant__ GhostArgs G) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= G.count) return;
-    const int sk = G.src[2 * e], sc = G.src[2 * e + 1];
+    if (e >= G.total) return;
+    const GhostSeg& S = G.segs[find_seg(G, e)];
+    const int le = e - S.start;
+    const int sk = S.src[2 * le], sc = S.src[2 * le + 1];
     const int kind = sk >> 24, sb = sk & 0xffffff;
     double q[5];
     if (kind == WM_SRC_CELL) {
-        const double* s = G.q[sb];
-        const long long n = G.ncell[sb];
+        const double* s = G.q[S.block0 + sb];
+        const long long n = G.ncell[S.block0 + sb];
 #pragma unroll
         for (int v = 0; v < 5; ++v) q[v] = s[v * n + sc];
     } else if (kind == WM_SRC_INFLOW) {
 #pragma unroll
-        for (int v = 0; v < 5; ++v) q[v] = G.inflow[v * G.inflow_n + sc];
+        for (int v = 0; v < 5; ++v) q[v] = S.inflow[v * S.inflow_n + sc];
     } else {
 #pragma unroll
-        for (int v = 0; v < 5; ++v) q[v] = G.bc[8 * sb + v];
+        for (int v = 0; v < 5; ++v) q[v] = S.bc[8 * sb + v];
     }
-    const int o0 = G.ops[2 * e], no = G.ops[2 * e + 1];
+    const int o0 = S.ops[2 * le], no = S.ops[2 * le + 1];
     for (int i = 0; i < no; ++i) {
-        const int code = G.op_code[o0 + i];
-        const double* nrm = G.op_nrm + 3 * (o0 + i);
-        const double* bc = G.bc + 8 * ((code >> 8) & 0xff);
+        const int code = S.op_code[o0 + i];
+        const double* nrm = S.op_nrm + 3 * (o0 + i);
+        const double* bc = S.bc + 8 * ((code >> 8) & 0xff);
         switch (code & 0xff) {
-            case WM_OP_SLIP: op_slip(q, nrm, G.gm1, G.Rg); break;
-            case WM_OP_NOSLIP: op_noslip(q, bc, G.gm1, G.Rg); break;
-            case WM_OP_FARFIELD: op_farfield(q, nrm, (code >> 16) & 1, bc, G.gamma, G.gm1, G.Rg); break;
+            case WM_OP_SLIP: op_slip(q, nrm, S.gm1, S.Rg); break;
+            case WM_OP_NOSLIP: op_noslip(q, bc, S.gm1, S.Rg); break;
+            case WM_OP_FARFIELD: op_farfield(q, nrm, (code >> 16) & 1, bc, S.gamma, S.gm1, S.Rg); break;
             default: break;
         }
     }
-    const int db = G.dst[2 * e], dc = G.dst[2 * e + 1];
+    const int db = S.block0 + S.dst[2 * le], dc = S.dst[2 * le + 1];
     if (G.stash != nullptr) {
         // two-phase mode: values first, scatter after every source has been read
 #pragma unroll
-        for (int v = 0; v < 5; ++v) G.stash[(long long)v * G.count + e] = q[v];
+        for (int v = 0; v < 5; ++v) G.stash[(long long)v * G.total + e] = q[v];
     } else {
         double* d = G.q[db];
         const long long n = G.ncell[db];
@@ -134,17 +146,19 @@ __global__ void ghost_gather_kernel(const __grid_constant__ GhostArgs G) {
 
 __global__ void ghost_scatter_kernel(const __grid_constant__ GhostArgs G) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= G.count) return;
-    const int db = G.dst[2 * e], dc = G.dst[2 * e + 1];
+    if (e >= G.total) return;
+    const GhostSeg& S = G.segs[find_seg(G, e)];
+    const int le = e - S.start;
+    const int db = S.block0 + S.dst[2 * le], dc = S.dst[2 * le + 1];
     double* d = G.q[db];
     const long long n = G.ncell[db];
 #pragma unroll
-    for (int v = 0; v < 5; ++v) d[v * n + dc] = G.stash[(long long)v * G.count + e];
+    for (int v = 0; v < 5; ++v) d[v * n + dc] = G.stash[(long long)v * G.total + e];
 }
 
 cudaError_t launch_ghost(const GhostArgs& G, cudaStream_t s) {
-    if (G.count == 0) return cudaSuccess;
-    const int nt = 256, nb = (G.count + nt - 1) / nt;
+    if (G.total == 0) return cudaSuccess;
+    const int nt = 256, nb = (G.total + nt - 1) / nt;
     ghost_gather_kernel<<<nb, nt, 0, s>>>(G);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || G.stash == nullptr) return e;

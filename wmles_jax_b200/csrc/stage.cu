@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
     };
 
     const int i0 = t.i0, i1 = t.i1;
-    const double dt = A.stage ? A.dt[B.case_id] : 0.0;
+    const double dt = A.stage ? *A.dt[B.case_id] : 0.0;
     double cmf_acc = 0.0;
 
     // ---- RK epilogue of interior cell (io, j, k): r = -(div F)/V (+ source), stage update
@@ -483,23 +483,28 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
         }
         __syncthreads();
         if (last) {
-            // the last tile sums the partials in a fixed order (run-to-run deterministic) and
-            // forms the shift delta = target - sum(rho u V) / sum(V), wmles/solver.py:24-29
+            // the last tile sums each case's partials over that case's tiles in a fixed order
+            // (the same alone or in a batch, run to run) and forms its shift
+            // delta = target - sum(rho u V) / sum(V), wmles/solver.py:24-29
             __threadfence();
             const volatile double* part = A.cmf_part;
-            double s = 0.0;
-            for (int i = tid; i < (int)gridDim.x; i += NT) s += part[i];
+            for (int c = 0; c < A.ncases; ++c) {
+                const CaseDev& Cc = A.cases[c];
+                const int t0 = A.case_tile_start[c], t1 = A.case_tile_start[c + 1];
+                double s = 0.0;
+                for (int i = t0 + tid; i < t1; i += NT) s += part[i];
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
-            __syncthreads();
-            if ((tid & 31) == 0) red[tid >> 5] = s;
-            __syncthreads();
-            if (tid == 0) {
-                double tot = 0.0;
-                for (int w = 0; w < NT / 32; ++w) tot += red[w];
-                A.cmf_delta[0] = C.cmf_target - tot / C.cmf_volume;
-                *A.cmf_counter = 0u;
+                for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+                __syncthreads();
+                if ((tid & 31) == 0) red[tid >> 5] = s;
+                __syncthreads();
+                if (tid == 0 && Cc.cmf_dir >= 0) {
+                    double tot = 0.0;
+                    for (int w = 0; w < NT / 32; ++w) tot += red[w];
+                    A.cmf_delta[c] = Cc.cmf_target - tot / Cc.cmf_volume;
+                }
             }
+            if (tid == 0) *A.cmf_counter = 0u;
         }
     }
 }

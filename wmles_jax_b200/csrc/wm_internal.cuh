@@ -1,4 +1,8 @@
 // Device-side descriptors shared by the kernels of libwmles_cuda.so.
+//
+// Every launch works on a *view*: a set of one or more independent cases whose blocks,
+// per-case constants, wall faces and stage tiles are concatenated into device tables.
+// Blocks carry a global index (into the view's block table) and their case's index.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -6,17 +10,19 @@
 
 namespace wm {
 
-// one structured block of a case, resident in device memory
+constexpr int MAX_CASES = WM_MAX_BLOCKS;   // a case has at least one block
+
+// one structured block, resident in device memory
 struct BlockDev {
     int n[3];          // interior cells
     int N[3];          // ghosted extents
     int ng;
-    int case_id;       // index into the CaseDev table
+    int case_id;       // index of the block's case in the view
     long long ncell;   // Ni*Nj*Nk
     long long plane;   // Nj*Nk
     const double* met;     // WM_NMET x ncell (float64)
     const float* met32;    // WM_NMET x ncell (float32 copy for the mixed form), may be null
-    int wall[6];       // wall index of face (axis*2 + side), -1 if not wall-modelled
+    int wall[6];       // view wall index of face (axis*2 + side), -1 if not wall-modelled
 };
 
 // per-case physical constants, precomputed where the kernels only need a derived value
@@ -26,6 +32,7 @@ struct CaseDev {
     double th0, inv_dth;   // Hybrid: s = clip((theta - th0) * inv_dth, 0, 1)
     double sgs_c;          // model coefficient
     double cfl, nu_fac;    // nu_fac = max(4/3, gamma/Pr)
+    double Pr13, Pr3, kader_beta;   // Pr^(1/3), Pr^3, (3.85 Pr^(1/3) - 1.3)^2 + 2.12 ln Pr
     int cmf_dir;
     double cmf_target, cmf_volume;
     int sponge;
@@ -33,7 +40,7 @@ struct CaseDev {
 };
 
 struct WallDev {
-    int block, axis, side, n_match;
+    int block, axis, side, n_match;   // block: view block index
     int isothermal, n_iter;
     int nt1, nt2;              // tangential interior extents (axes in increasing order)
     double T_wall, kappa, B, ekb;
@@ -44,7 +51,22 @@ struct WallDev {
 
 // stage-kernel work item: one (j,k) tile of one block over planes [i0, i1)
 struct Tile {
-    int blk, j0, k0, i0, i1;
+    int blk, j0, k0, i0, i1;   // blk: view block index
+};
+
+// one case's ghost-cell program inside a view-wide gather launch
+struct GhostSeg {
+    const int* dst;
+    const int* src;
+    const int* ops;
+    const int* op_code;
+    const double* op_nrm;
+    const double* bc;          // the case's BC table (8 per BC)
+    const double* inflow;      // 5 x inflow_n (or null)
+    long long inflow_n;
+    int start, count;          // entries [start, start + count) of the launch
+    int block0;                // view index of the case's first block
+    double gamma, gm1, Rg;
 };
 
 struct StatePtrs {
@@ -63,11 +85,13 @@ struct StageArgs {
     const WallDev* walls;
     const Tile* tiles;
     int ntiles;
-    int stage;              // 0: q_out = RHS; 1,2,3: SSP-RK3 stage
-    const double* dt;       // device time step (per case: dt[case_id])
-    double* cmf_part;       // stage 3 with constant mass flux: per-tile partial sums
-    unsigned int* cmf_counter;  // last-CTA-done counter (the last CTA resets it)
-    double* cmf_delta;      // constant-mass-flux shift, written by the last CTA
+    int stage;                    // 0: q_out = RHS; 1,2,3: SSP-RK3 stage
+    int ncases;
+    const int* case_tile_start;   // ncases + 1: tiles of case c are [start[c], start[c+1])
+    double* cmf_part;             // stage 3 with constant mass flux: per-tile partial sums
+    unsigned int* cmf_counter;    // last-CTA-done counter (the last CTA resets it)
+    double* cmf_delta;            // per case: constant-mass-flux shift, written by the last CTA
+    const double* dt[MAX_CASES];  // per case: device time step
     StatePtrs p[WM_MAX_BLOCKS];
 };
 

@@ -30,8 +30,27 @@ SRC_CELL, SRC_INFLOW, SRC_CONST = 0, 1, 2
 _K_INFLOW, _K_CONST, _K_OP = 1, 2, 3
 
 
+_SHARED = {}   # id(geom) -> [geom, packed metrics or None], for geometries many cases reuse
+
+
+def share_metrics(mesh):
+    """Keep the packed metric arrays of `mesh` after their first use (for a mesh shared by
+    many cases, e.g. a serving grid cache); the registry holds the mesh's geometries."""
+    for g in mesh.geoms:
+        _SHARED.setdefault(id(g), [g, None])
+
+
 def block_metrics(blk, geom):
     """(NMET, Ni, Nj, Nk) float64 metric array of one block."""
+    ent = _SHARED.get(id(geom))
+    if ent is not None and ent[0] is geom:
+        if ent[1] is None:
+            ent[1] = _block_metrics(blk, geom)
+        return ent[1]
+    return _block_metrics(blk, geom)
+
+
+def _block_metrics(blk, geom):
     Ni, Nj, Nk = blk.N
     M = np.empty((NMET, Ni, Nj, Nk))
     M[0:3] = geom.S[0][:, :Ni]

@@ -1,0 +1,391 @@
+"""Continuous batching of many independent cases on one GPU.
+
+A *request* is one case (mesh, gas, solver options, initial condition) to be advanced a
+fixed number of steps; its result is the final state.  Requests arrive at any time.  The
+server keeps every admitted case resident in HBM (metrics, ghost programs, two state
+buffers used in ping-pong, two device time steps) and advances ALL resident cases together:
+one ``wm_batch_step`` per step, i.e. one launch per kernel per RK stage over the
+concatenated block / tile work list of every case (libwmles_cuda.so, wm_batch_*).  While the
+set of resident cases stays the same, each step is replayed from a CUDA graph (two graphs,
+one per ping-pong parity).  Between steps the server retires finished cases and admits
+waiting ones, so requests that arrive while others run join the next step.
+
+* Admission: a request is admitted when its estimated device bytes fit in the free HBM
+  (device free memory plus what PyTorch's allocator holds unused) minus a reserve, and the
+  batch has block slots left (at most ``WM_MAX_BLOCKS`` blocks per batch).
+* Host preparation (mesh, metrics, ghost programs, initial state) runs on a builder thread,
+  overlapping the GPU steps; graph captures and case construction exclude each other.
+* Results do not depend on the mix: per-case reductions run over that case's own cells in
+  a fixed order and its stage tiles are fixed at construction, so a case advanced in any
+  batch is bit-identical to the same case advanced alone with ``Solver.step``.
+* Time-to-result is measured from the request's arrival to the moment the host sees the
+  device finish the request's last step (an event per step, at most two steps in flight).
+
+No reference counterpart: the reference advances one case per ``Solver`` in a Python loop
+(examples/channel_wmles.py:121-152).
+"""
+import ctypes as C
+import queue
+import threading
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _native as N
+from .lowering import NMET
+
+
+# ---------------------------------------------------------------------------- batch handle
+class Batch:
+    """A wm_batch over solvers that share precision, scheme, SGS model and tile shape."""
+
+    def __init__(self, solvers):
+        self.solvers = list(solvers)
+        if not self.solvers:
+            raise ValueError("a batch needs at least one solver")
+        self._lib = N.load()
+        arr = (C.c_void_p * len(self.solvers))(*[s._case.value for s in self.solvers])
+        h = C.c_void_p()
+        N.check(self._lib.wm_batch_create(len(self.solvers), arr, C.byref(h)), "wm_batch_create")
+        self._h = h
+        nb, nt, nl = C.c_int(), C.c_int(), C.c_longlong()
+        N.check(self._lib.wm_batch_info(h, C.byref(nb), C.byref(nt), C.byref(nl)), "wm_batch_info")
+        self.nblocks, self.ntiles, self.launches_per_step = nb.value, nt.value, nl.value
+
+    def args(self, q_in, q_out, dt_in, dt_next, times=None):
+        """Pointer arrays of one step: q_in/q_out are per-solver state tuples, dt_* per-solver
+        0-d float64 tensors.  Built once per membership and parity, replayed many times."""
+        flat = lambda qs: N.ptr_array([q.data_ptr() for Q in qs for q in Q])  # noqa: E731
+        t = np.zeros(len(self.solvers)) if times is None else np.asarray(times, dtype=np.float64)
+        return (flat(q_in), flat(q_out), N.ptr_array([d.data_ptr() for d in dt_in]),
+                N.ptr_array([d.data_ptr() for d in dt_next]), np.ascontiguousarray(t))
+
+    def step_args(self, args, stream=None):
+        qi, qo, di, dn, t = args
+        s = C.c_void_p((stream or torch.cuda.current_stream()).cuda_stream)
+        N.check(self._lib.wm_batch_step(self._h, qi, qo, di, dn, N.as_double_p(t), s), "wm_batch_step")
+
+    def step(self, q_in, q_out, dt_in, dt_next, times=None, stream=None):
+        self.step_args(self.args(q_in, q_out, dt_in, dt_next, times), stream)
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.wm_batch_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # pragma: no cover - interpreter shutdown
+            pass
+
+
+# ---------------------------------------------------------------------------- requests
+@dataclass
+class Request:
+    """One case to advance ``steps`` steps.  ``build()`` returns (mesh, gas, solver kwargs,
+    prim_fn) like workloads.channel_case; ``dims`` are the interior extents of its blocks
+    (known before building, used for admission)."""
+    rid: int
+    build: object
+    steps: int
+    arrival: float = 0.0                  # seconds after the server starts
+    dims: tuple = ()
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def cells(self):
+        return int(sum(np.prod(d) for d in self.dims))
+
+
+def estimate_bytes(dims, precision, ng=3):
+    """Device bytes of a resident case: FP64 metrics (+ FP32 copy for the mixed form), two
+    work states of the RK stages, two ping-pong states, plus 10 % for wall faces, ghost
+    programs and tables."""
+    met = NMET * (8 + (4 if precision == "mixed" else 0))
+    per_cell = met + 2 * 40 + 2 * 40
+    cells = sum(int(np.prod([n + 2 * ng for n in d])) for d in dims)
+    return int(1.1 * per_cell * cells) + (1 << 20)
+
+
+def free_device_bytes(device=None):
+    free, _ = torch.cuda.mem_get_info(device)
+    return free + torch.cuda.memory_reserved(device) - torch.cuda.memory_allocated(device)
+
+
+class Admission:
+    """Admission bookkeeping: bytes reserved by admitted-but-unbuilt or resident cases are
+    charged against a budget measured once at start (device free bytes minus a reserve), so
+    decisions do not race with allocations in flight."""
+
+    def __init__(self, budget_bytes, max_blocks=N.MAX_BLOCKS, max_cases=N.MAX_BLOCKS):
+        self.budget, self.max_blocks, self.max_cases = int(budget_bytes), max_blocks, max_cases
+        self.used = 0
+        self.blocks = 0
+        self.cases = 0
+        self.peak = 0             # most bytes ever charged at once
+
+    def fits(self, nbytes, nblocks):
+        if nbytes > self.budget or nblocks > self.max_blocks:
+            raise ValueError(f"request needs {nbytes} bytes / {nblocks} blocks: it can never be admitted "
+                             f"(budget {self.budget} bytes, {self.max_blocks} blocks)")
+        return (self.used + nbytes <= self.budget and self.blocks + nblocks <= self.max_blocks
+                and self.cases + 1 <= self.max_cases)
+
+    def take(self, nbytes, nblocks):
+        self.used += nbytes
+        self.peak = max(self.peak, self.used)
+        self.blocks += nblocks
+        self.cases += 1
+
+    def give(self, nbytes, nblocks):
+        self.used -= nbytes
+        self.blocks -= nblocks
+        self.cases -= 1
+
+
+@dataclass
+class _Resident:
+    req: Request
+    solver: object
+    bufs: list            # [state A, state B], tuples of per-block tensors
+    dts: list             # [dt A, dt B], 0-d float64 tensors
+    nbytes: int
+    parity: int = 0       # bufs[parity] holds the current state
+    done: int = 0         # steps completed
+    admitted: float = 0.0
+
+
+@dataclass
+class Result:
+    rid: int
+    state: tuple          # final state (device tensors)
+    dt: torch.Tensor      # CFL time step of the final state (device)
+    steps: int
+    cells: int
+    arrival: float
+    admitted: float
+    finished: float
+
+    @property
+    def time_to_result(self):
+        return self.finished - self.arrival
+
+
+# ---------------------------------------------------------------------------- server
+class Server:
+    """Continuous-batching server (see the module docstring).
+
+    precision / tile / chunk: solver options shared by every case (one batch); graphs: replay
+    steps from CUDA graphs once a membership has run ``graph_after`` steps eagerly;
+    reserve_bytes: HBM left free; budget_bytes: override of the admission budget."""
+
+    def __init__(self, precision="mixed", tile=None, chunk=None, graphs=True, graph_after=2,
+                 reserve_bytes=4 << 30, budget_bytes=None, device=None):
+        from .backend import require_gpu
+        self.device = device or require_gpu()
+        self.precision, self.tile, self.chunk = precision, tile, chunk
+        self.graphs, self.graph_after = graphs, graph_after
+        budget = budget_bytes if budget_bytes is not None else free_device_bytes(self.device) - reserve_bytes
+        self.admission = Admission(max(0, budget))
+        self.stream = torch.cuda.Stream(self.device)
+        self._lock = threading.Lock()             # case construction vs graph capture
+        self._cond = threading.Condition()        # admission waits for retirements
+        self.stats = {}
+
+    # ------------------------------------------------------------------ building
+    def _build(self, req, bstream):
+        from .solver import Solver
+        mesh, gas, kw, prim = req.build()
+        for src in kw.get("sources", ()):
+            if hasattr(src, "fill_at_time"):
+                raise NotImplementedError("the server advances time-independent cases only")
+        with self._lock, torch.cuda.stream(bstream):
+            solver = Solver(mesh, gas, precision=self.precision, tile=self.tile, chunk=self.chunk, **kw)
+            if solver.has_inflow:
+                raise NotImplementedError("the server advances cases without a synthetic inflow only")
+            qa = solver.init_state(prim)
+            qb = tuple(torch.empty_like(q) for q in qa)
+            da = solver.max_dt(qa)
+            db = torch.empty_like(da)
+            bstream.synchronize()
+        return solver, [qa, qb], [da, db]
+
+    def _builder(self, requests, t0, ready, errors):
+        bstream = torch.cuda.Stream(self.device)
+        try:
+            for req in requests:
+                delay = t0 + req.arrival - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                nbytes = estimate_bytes(req.dims, self.precision)
+                with self._cond:
+                    while not self.admission.fits(nbytes, len(req.dims)):
+                        self._cond.wait(timeout=0.05)
+                    self.admission.take(nbytes, len(req.dims))
+                solver, bufs, dts = self._build(req, bstream)
+                ready.put(_Resident(req, solver, bufs, dts, nbytes, admitted=time.perf_counter() - t0))
+        except BaseException as e:   # surfaced by run()
+            errors.append(e)
+        finally:
+            ready.put(None)
+
+    # ------------------------------------------------------------------ stepping
+    def _capture(self, batch, args):
+        """CUDA graph of one batch step, or None while the builder thread holds the device
+        (case construction allocates and synchronises, which a capture must not see)."""
+        if not self._lock.acquire(blocking=False):
+            return None
+        try:
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=self.stream, capture_error_mode="thread_local"):
+                batch.step_args(args, self.stream)
+            return g
+        finally:
+            self._lock.release()
+
+    def run(self, requests, timeout=None):
+        """Serve ``requests`` (arrival times relative to now); returns {rid: Result}."""
+        requests = sorted(requests, key=lambda r: r.arrival)
+        ready, errors = queue.Queue(), []
+        t0 = time.perf_counter()
+        builder = threading.Thread(target=self._builder, args=(requests, t0, ready, errors), daemon=True)
+        builder.start()
+        active, joined, results = [], [], {}
+        pending = []               # (event, [residents finished by that step]) of steps in flight
+        batch, args, graphs, run_len = None, {}, {}, 0
+        builder_done = False
+        n = dict(batch_steps=0, graph_steps=0, captures=0, memberships=0, kernel_launches=0, cell_steps=0)
+
+        def clock():
+            return time.perf_counter() - t0
+
+        def take(item):
+            nonlocal builder_done
+            if item is None:
+                builder_done = True
+            else:
+                joined.append(item)
+
+        def stamp(upto):
+            while len(pending) > upto:
+                ev, fin = pending.pop(0)
+                ev.synchronize()
+                now = clock()
+                for r in fin:
+                    results[r.req.rid] = Result(r.req.rid, r.bufs[r.parity], r.dts[r.parity], r.done,
+                                                r.req.cells, r.req.arrival, r.admitted, now)
+
+        def release(rs):
+            with self._cond:
+                for r in rs:
+                    r.bufs[1 - r.parity] = None
+                    r.dts[1 - r.parity] = None
+                    r.solver = None
+                    self.admission.give(r.nbytes, len(r.req.dims))
+                self._cond.notify_all()
+
+        with torch.cuda.stream(self.stream):
+            while True:
+                if errors:
+                    raise errors[0]
+                if timeout is not None and clock() > timeout:
+                    raise TimeoutError("serving did not finish in time")
+                if not active and not joined and not builder_done:
+                    try:                       # idle: wait for the next admitted case
+                        take(ready.get(timeout=0.05))
+                    except queue.Empty:
+                        continue
+                while True:                    # every case admitted since the last step
+                    try:
+                        take(ready.get_nowait())
+                    except queue.Empty:
+                        break
+                leaving = [r for r in active if r.done >= r.req.steps]
+                if joined or leaving or (batch is None and active):
+                    # membership change: drain the steps in flight, free the leavers, rebuild
+                    self.stream.synchronize()
+                    stamp(0)
+                    graphs.clear()
+                    args = {}
+                    if batch is not None:
+                        batch.close()
+                        batch = None
+                    active = [r for r in active if r.done < r.req.steps]
+                    release(leaving)
+                    for r in joined:
+                        if r.req.steps <= 0:
+                            results[r.req.rid] = Result(r.req.rid, r.bufs[0], r.dts[0], 0, r.req.cells,
+                                                        r.req.arrival, r.admitted, clock())
+                            release([r])
+                        else:
+                            active.append(r)
+                    joined = []
+                    if active:
+                        batch = Batch([r.solver for r in active])
+                        n["memberships"] += 1
+                        run_len = 0
+                if not active:
+                    if builder_done and ready.empty():
+                        break
+                    continue
+                key = tuple(r.parity for r in active)
+                if key not in args:
+                    args[key] = batch.args([r.bufs[r.parity] for r in active],
+                                           [r.bufs[1 - r.parity] for r in active],
+                                           [r.dts[r.parity] for r in active],
+                                           [r.dts[1 - r.parity] for r in active])
+                g = graphs.get(key)
+                if g is None and self.graphs and run_len >= self.graph_after:
+                    g = self._capture(batch, args[key])
+                    if g is not None:
+                        graphs[key] = g
+                        n["captures"] += 1
+                if g is not None:
+                    g.replay()
+                    n["graph_steps"] += 1
+                else:
+                    batch.step_args(args[key], self.stream)
+                run_len += 1
+                n["batch_steps"] += 1
+                n["kernel_launches"] += batch.launches_per_step
+                fin = []
+                for r in active:
+                    r.parity ^= 1
+                    r.done += 1
+                    n["cell_steps"] += r.req.cells
+                    if r.done >= r.req.steps:
+                        fin.append(r)
+                ev = torch.cuda.Event()
+                ev.record(self.stream)
+                pending.append((ev, fin))
+                stamp(2)                       # at most two steps in flight
+            self.stream.synchronize()
+            stamp(0)
+            if batch is not None:
+                batch.close()
+        builder.join()
+        if errors:
+            raise errors[0]
+        wall = max((r.finished for r in results.values()), default=0.0)
+        ttr = np.array([r.time_to_result for r in results.values()])
+        self.stats = dict(n, requests=len(results), wall_s=wall, peak_admitted_bytes=self.admission.peak,
+                          mcell_steps_per_s=n["cell_steps"] / wall / 1e6 if wall > 0 else 0.0,
+                          p50_s=float(np.percentile(ttr, 50)) if len(ttr) else None,
+                          p99_s=float(np.percentile(ttr, 99)) if len(ttr) else None)
+        return results
+
+
+# ---------------------------------------------------------------------------- helpers
+def serve_alone(req, precision="mixed", tile=None, chunk=None):
+    """The request advanced by itself through Solver.step (the reference loop); returns
+    (state, dt of the final state)."""
+    from .solver import Solver
+    mesh, gas, kw, prim = req.build()
+    s = Solver(mesh, gas, precision=precision, tile=tile, chunk=chunk, **kw)
+    Q = s.init_state(prim)
+    for _ in range(req.steps):
+        Q, _ = s.step(Q)
+    return Q, s.max_dt(Q)

@@ -153,6 +153,7 @@ class Solver:
                     inf.U_inf, inf.L, inf.rho_inf, inf.p_inf = p["U_inf"], p["L"], p["rho_inf"], p["p_inf"]
                     self._keep.append(inf)
                     d.inflow = C.pointer(inf)
+        self.has_inflow = bool(d.inflow)
         # sources
         d.sponge.enabled = 0
         for src in self.sources:

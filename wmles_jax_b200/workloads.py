@@ -11,6 +11,8 @@
 
 No external data: every input is generated here from formulas and a NumPy seed.
 """
+import functools
+
 import numpy as np
 
 from .bc import WallModel
@@ -118,3 +120,53 @@ def channel_case(config=2, n=None, blocks=None):
 STAGE_BYTES = {"fp64": (184, 224, 224), "mixed": (132, 172, 172)}
 STEP_BYTES = {"fp64": 752, "mixed": 556}
 CMF_BYTES = 80
+
+
+# ---------------------------------------------------------------------------- serving mix
+SERVING_GRIDS = ((48, 48, 48), (64, 48, 48), (96, 64, 64), (128, 96, 64), (192, 96, 96))
+
+
+def re_bulk_from_re_tau(re_tau):
+    """Half-height bulk Reynolds number for a friction Reynolds number, from Dean's
+    correlation Re_tau = 0.09 Re_m^0.88 with Re_m = U_b (2h) / nu on the full height."""
+    return 0.5 * (np.asarray(re_tau, dtype=float) / 0.09) ** (1.0 / 0.88)
+
+
+@functools.lru_cache(maxsize=16)
+def serving_mesh(grid):
+    """Finalized channel mesh of one serving grid, built once and shared by every request on
+    that grid (the geometry does not depend on Re_tau or Ma_b); its packed metrics are kept."""
+    from .lowering import share_metrics
+    mesh = channel_mesh(grid, blocks=1, beta=2.5)
+    share_metrics(mesh)
+    return mesh
+
+
+def serving_case(re_tau, ma_b, grid, seed=0):
+    """(mesh, gas, solver kwargs, prim_fn) of one serving request: the config-2 channel
+    (tanh stretching beta = 2.5, KEP4 + WALE 0.5, wall model at the 3rd cell, constant
+    mass flux, CFL 0.5) at the given Re_tau, bulk Mach number and grid, log-law IC with
+    seeded noise."""
+    gas = channel_gas(Ma_b=float(ma_b), Re_b=float(re_bulk_from_re_tau(re_tau)))
+    mesh = serving_mesh(tuple(int(n) for n in grid))
+    kw = dict(scheme=KEP(4), sgs="wale", sgs_kwargs=dict(Cw=0.5), cfl=0.5,
+              constraints=[ConstantMassFlux(0, 1.0)])
+    return mesh, gas, kw, loglaw_prim(gas, mesh, seed=seed)
+
+
+def serving_requests(n=64, rate=20.0, steps=2000, seed=0, grids=SERVING_GRIDS):
+    """Seeded request mix: Poisson arrivals at `rate` per second, Re_tau ~ U[550, 5200],
+    Ma_b ~ U[0.1, 0.5], grid drawn uniformly from `grids`; request r's IC noise uses seed r."""
+    from .serving import Request
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+    re_tau = rng.uniform(550.0, 5200.0, n)
+    ma_b = rng.uniform(0.1, 0.5, n)
+    gidx = rng.integers(0, len(grids), n)
+    out = []
+    for r in range(n):
+        grid, rt, ma = grids[gidx[r]], float(re_tau[r]), float(ma_b[r])
+        out.append(Request(rid=r, build=(lambda rt=rt, ma=ma, grid=grid, r=r: serving_case(rt, ma, grid, seed=r)),
+                           steps=int(steps), arrival=float(arrivals[r]), dims=(tuple(grid),),
+                           meta=dict(re_tau=rt, ma_b=ma, grid=tuple(grid))))
+    return out
