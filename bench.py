@@ -15,6 +15,9 @@ mixed       the mixed-precision form (FP32 fluxes/gradients/SGS, FP64 state and 
 roofline    the fused stage kernel: algorithmic bytes per launch / mean launch time
 cpu_baseline  the CPU oracle (NumPy float64 restatement of the reference) on a slab of the
             same workload, one core
+serving     config 5: 64 seeded channel requests (Poisson arrivals at 20/s; uneven grids, Re_tau,
+            Ma_b), mixed precision, 2000 steps each, continuously batched on one GPU: p50/p99
+            time-to-result and aggregate Mcell-steps/s (--serving-requests 0 skips it)
 --impl reference  the oracle on the host cores (one process per core, each on its own slab)
 """
 import argparse
@@ -234,9 +237,48 @@ def run_ours(args, rank, world, local_rank):
     }
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.cpu_cells)
+    if world == 1 and args.serving_requests > 0:
+        del s64, s32, Q64, Q32, Qn, dbuf
+        line["serving"] = serving_leg(args)
     if dist is not None:
         dist.destroy_process_group()
     return line
+
+
+# ----------------------------------------------------------------------------- serving (config 5)
+def serving_leg(args):
+    """Continuous batching of seeded channel requests (Poisson arrivals, uneven grids, Re_tau and
+    Ma_b), mixed precision; p50/p99 time-to-result and aggregate Mcell-steps/s."""
+    import torch
+    from wmles_jax_b200.lowering import block_metrics
+    from wmles_jax_b200.serving import Server
+    from wmles_jax_b200.workloads import SERVING_GRIDS, serving_mesh, serving_requests
+    for g in SERVING_GRIDS:                 # grid catalogue: meshes and metrics built at server start
+        m = serving_mesh(g)
+        for b, geo in zip(m.blocks, m.geoms):
+            block_metrics(b, geo)
+    reqs = serving_requests(n=args.serving_requests, rate=args.serving_rate, steps=args.serving_steps, seed=0)
+    torch.cuda.synchronize()
+    srv = Server(precision="mixed", graphs=True, tile="auto", policy="sjf")
+    tile, tile_ms = srv.tune(reqs)              # before the arrivals start (cached per machine)
+    srv.tile = tile
+    results = srv.run(reqs, timeout=1800)
+    st = srv.stats
+    bad = sum(1 for r in results.values() if not all(bool(torch.isfinite(q).all()) for q in r.state))
+    return {"requests": st["requests"], "steps_per_request": args.serving_steps,
+            "arrivals": f"Poisson, {args.serving_rate}/s, seed 0",
+            "grids": [list(g) for g in SERVING_GRIDS], "re_tau": [550, 5200], "ma_b": [0.1, 0.5],
+            "form": "mixed", "admission": "shortest job first, 8M-cell resident budget, free-HBM check",
+            "tile": tile, "tile_ms_per_step": tile_ms,
+            "p50_time_to_result_s": st["p50_s"], "p99_time_to_result_s": st["p99_s"],
+            "value": st["mcell_steps_per_s"], "unit": METRIC, "wall_s": st["wall_s"],
+            "device_busy_s": st["device_busy_s"], "device_value": st["device_mcell_steps_per_s"],
+            "cell_steps": st["cell_steps"], "batch_steps": st["batch_steps"], "graph_steps": st["graph_steps"],
+            "graph_captures": st["captures"], "memberships": st["memberships"],
+            "gpu_launches": st["kernel_launches"], "peak_admitted_bytes": st["peak_admitted_bytes"],
+            "nonfinite_results": bad,
+            "time_to_result": "arrival to the host seeing the last step done on the device, including "
+                              "host-side case preparation (IC, ghost programs) and admission"}
 
 
 # ----------------------------------------------------------------------------- CPU oracle
@@ -300,6 +342,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-cells", type=int, default=8, help="x-cells of the CPU slab sample")
     ap.add_argument("--max-workers", type=int, default=64)
+    ap.add_argument("--serving-requests", type=int, default=64, help="config-5 requests (0: skip the leg)")
+    ap.add_argument("--serving-steps", type=int, default=2000)
+    ap.add_argument("--serving-rate", type=float, default=20.0)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")

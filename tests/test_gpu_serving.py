@@ -95,3 +95,34 @@ def test_server_admission_budget():
     _check_server(results, reqs, alone)
     assert srv.stats["peak_admitted_bytes"] <= budget
     assert srv.stats["memberships"] >= 3
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_results_do_not_depend_on_chunk(precision):
+    """The stage work list may be cut into any chunk length along i (a batch picks its own):
+    the constant-mass-flux partials are per column and plane, so results are bit-identical."""
+    from wmles_jax_b200 import Solver
+    from wmles_jax_b200.workloads import serving_case
+    outs = []
+    for chunk in (None, 4, 7, 24):
+        # a fresh builder per run: prim_fn draws its noise from a generator it owns
+        mesh, gas, kw, prim = serving_case(1500.0, 0.3, (24, 16, 16), seed=5)
+        s = Solver(mesh, gas, precision=precision, chunk=chunk, **kw)
+        Q = s.init_state(prim)
+        for _ in range(4):
+            Q, dt = s.step(Q)
+        outs.append((Q, s.max_dt(Q)))
+    for Q, dt in outs[1:]:
+        assert _same(Q, outs[0][0]) and torch.equal(dt, outs[0][1])
+
+
+def test_autotune_picks_a_measured_tile(tmp_path, monkeypatch):
+    from wmles_jax_b200 import autotune
+    from wmles_jax_b200.workloads import serving_case
+    monkeypatch.setenv("WMLES_TUNE_CACHE", str(tmp_path / "tiles.json"))
+    cases = [serving_case(800.0, 0.3, g, seed=1) for g in ((16, 16, 16), (24, 16, 16))]
+    tile, ms = autotune.tune(cases, precision="mixed", steps=4, warmup=3)
+    assert set(ms) == set(autotune.CANDIDATES["mixed"]) and tile == autotune.pick(ms)
+    assert all(v > 0 for v in ms.values())
+    tile2, ms2 = autotune.tune(cases, precision="mixed")     # served from the cache
+    assert tile2 == tile and ms2 == ms

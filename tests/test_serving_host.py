@@ -3,7 +3,7 @@ estimate, the seeded request mix and the Re_tau -> Re_b mapping."""
 import numpy as np
 import pytest
 
-from wmles_jax_b200.serving import Admission, estimate_bytes
+from wmles_jax_b200.serving import Admission, Request, estimate_bytes, pick_next
 from wmles_jax_b200.workloads import SERVING_GRIDS, re_bulk_from_re_tau, serving_requests
 
 
@@ -21,6 +21,35 @@ def test_admission_accounting():
         a.fits(2000, 1)                # can never be admitted
     with pytest.raises(ValueError):
         a.fits(10, 4)
+
+
+def test_admission_cell_budget():
+    a = Admission(1 << 40, max_cells=100)
+    assert a.fits(1, 1, 500)             # an empty server admits any case whose bytes fit
+    a.take(1, 1, 500)
+    assert not a.fits(1, 1, 1)
+    a.give(1, 1, 500)
+    a.take(1, 1, 60)
+    assert a.fits(1, 1, 40) and not a.fits(1, 1, 41)
+
+
+def _req(rid, dims, steps, arrival):
+    return Request(rid=rid, build=None, steps=steps, arrival=arrival, dims=(dims,))
+
+
+def test_pick_next_policies():
+    big, small, mid = _req(0, (40, 40, 40), 10, 0.0), _req(1, (8, 8, 8), 10, 0.5), _req(2, (20, 20, 20), 10, 0.2)
+    waiting = [big, small, mid]
+    a = Admission(1 << 40)
+    assert pick_next(waiting, a, "mixed", "sjf") is small
+    assert pick_next(waiting, a, "mixed", "fifo") is big
+    # sjf backfills with whatever fits; fifo does not skip the head of the queue
+    a = Admission(1 << 40, max_cells=9000)
+    a.take(1, 1, 1)
+    assert pick_next([big, mid], a, "mixed", "sjf") is mid
+    assert pick_next([big, mid], a, "mixed", "fifo") is None
+    with pytest.raises(ValueError):
+        pick_next(waiting, a, "mixed", "lifo")
 
 
 def test_estimate_bytes():

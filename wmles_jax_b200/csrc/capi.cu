@@ -5,9 +5,11 @@
 // (blocks, per-case constants, wall faces, stage tiles, ghost-program segments) and the
 // reduction scratch of a set of cases.  Every wm_case carries a View of itself for the
 // single-case entry points; a wm_batch is a View over several resident cases, so one
-// launch per kernel and stage advances all of them.  Per-case reductions (CFL minimum,
-// constant-mass-flux sum) run over each case's own CTAs / tiles in a fixed order, so a
-// case's result does not depend on what else is in the batch.
+// launch per kernel and stage advances all of them.  The stage work list is cut for the
+// whole view (longer chunks along i when many cases share the GPU).  Per-case reductions
+// (CFL minimum; constant-mass-flux sum over fixed per-column, per-plane, per-warp partials)
+// run in a fixed order, so a case's result depends neither on the chunk length nor on what
+// else is in the batch.
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
@@ -140,7 +142,7 @@ struct wm_case {
     std::vector<BlockDev> hb;
     CaseDev hc{};
     std::vector<WallDev> hw;
-    std::vector<Tile> tiles;
+    int chunk_req = 0;                   // planes per stage-kernel CTA requested (0: automatic)
     StageOpts opts{};
     std::vector<double*> work[2];
     GhostProg prog_rhs, prog_all;
@@ -166,15 +168,16 @@ struct View {
     std::vector<BlockDev> hb;
     std::vector<CaseDev> hc;
     std::vector<WallDev> hw;
-    std::vector<Tile> tiles;
-    std::vector<int> case_tile_start, case_block_start;
+    std::vector<Tile> tiles;             // stage work list: (j,k) columns of every block, cut along i
+    std::vector<int> case_block_start;
+    std::vector<int> cmf_slot_start, case_slot_start;   // constant-mass-flux partial slots
     std::vector<GhostSeg> seg_rhs, seg_all;
     int total_rhs = 0, total_all = 0;
     BlockDev* d_blocks = nullptr;
     CaseDev* d_cases = nullptr;
     WallDev* d_walls = nullptr;
     Tile* d_tiles = nullptr;
-    int* d_case_tile_start = nullptr;
+    int* d_case_slot_start = nullptr;
     GhostSeg *d_seg_rhs = nullptr, *d_seg_all = nullptr;
     double *cmf_part = nullptr, *cmf_delta = nullptr, *dt_part = nullptr;
     unsigned* counters = nullptr;        // [0]: CFL reduction, [1]: constant-mass-flux reduction
@@ -251,16 +254,25 @@ int choose_chunk(const std::vector<BlockDev>& hb, const StageOpts& opts, int tj,
     return best_ic;
 }
 
-void build_tiles(wm_case* c, int tj, int tk, int ic) {
-    c->tiles.clear();
-    for (int b = 0; b < (int)c->hb.size(); ++b) {
-        const BlockDev& B = c->hb[b];
+// stage work list of a view: every (j,k) column of every block, cut into chunks of ic planes;
+// plus the constant-mass-flux partial slots, one per (column, interior plane, warp) of each
+// block, which do not depend on ic
+void build_tiles(View* v, int tj, int tk, int ic) {
+    v->tiles.clear();
+    v->cmf_slot_start.assign(1, 0);
+    const int warps = tj * tk / 32;
+    for (int b = 0; b < v->nblocks; ++b) {
+        const BlockDev& B = v->hb[b];
         const int ng = B.ng;
         for (int i0 = ng; i0 < ng + B.n[0]; i0 += ic)
             for (int j0 = ng; j0 < ng + B.n[1]; j0 += tj)
                 for (int k0 = ng; k0 < ng + B.n[2]; k0 += tk)
-                    c->tiles.push_back(Tile{b, j0, k0, i0, std::min(i0 + ic, ng + B.n[0])});
+                    v->tiles.push_back(Tile{b, j0, k0, i0, std::min(i0 + ic, ng + B.n[0])});
+        const int cols = ((B.n[1] + tj - 1) / tj) * ((B.n[2] + tk - 1) / tk);
+        v->cmf_slot_start.push_back(v->cmf_slot_start.back() + cols * B.n[0] * warps);
     }
+    v->case_slot_start.clear();
+    for (int c = 0; c <= v->ncases; ++c) v->case_slot_start.push_back(v->cmf_slot_start[v->case_block_start[c]]);
 }
 
 bool same_opts(const StageOpts& a, const StageOpts& b) {
@@ -292,7 +304,6 @@ int build_view(View* v, wm_case* const* cases, int n) {
             return fail(WM_E_UNSUPPORTED, "a batch holds at most %d blocks", WM_MAX_BLOCKS);
         v->members.push_back(c);
         v->case_block_start.push_back(bo);
-        v->case_tile_start.push_back((int)v->tiles.size());
         for (BlockDev B : c->hb) {
             B.case_id = ci;
             for (int f = 0; f < 6; ++f)
@@ -305,10 +316,6 @@ int build_view(View* v, wm_case* const* cases, int n) {
             v->hw.push_back(W);
         }
         v->hc.push_back(c->hc);
-        for (Tile t : c->tiles) {
-            t.blk += bo;
-            v->tiles.push_back(t);
-        }
         v->seg_rhs.push_back(segment(c, c->prog_rhs, v->total_rhs, bo));
         v->total_rhs += c->prog_rhs.count;
         v->seg_all.push_back(segment(c, c->prog_all, v->total_all, bo));
@@ -319,10 +326,16 @@ int build_view(View* v, wm_case* const* cases, int n) {
         v->any_cmf = v->any_cmf || c->hc.cmf_dir >= 0;
     }
     v->case_block_start.push_back((int)v->hb.size());
-    v->case_tile_start.push_back((int)v->tiles.size());
     v->nblocks = (int)v->hb.size();
     v->ncases = n;
     v->opts = cases[0]->opts;
+    // the chunk length is chosen for the whole set (results do not depend on it)
+    int req = cases[0]->chunk_req;
+    for (int ci = 1; ci < n; ++ci)
+        if (cases[ci]->chunk_req != req) req = 0;
+    int tj, tk;
+    tile_shape(v->opts.tile, &tj, &tk);
+    build_tiles(v, tj, tk, choose_chunk(v->hb, v->opts, tj, tk, req));
     v->cta_start.assign(1, 0);                  // one interior cell per thread of the CFL pass
     for (const BlockDev& B : v->hb)
         v->cta_start.push_back(v->cta_start.back() + (int)(((long long)B.n[0] * B.n[1] * B.n[2] + DT_NT - 1) / DT_NT));
@@ -332,10 +345,10 @@ int build_view(View* v, wm_case* const* cases, int n) {
     if ((r = m.upload(&v->d_cases, v->hc.data(), v->hc.size()))) return r;
     if ((r = m.upload(&v->d_walls, v->hw.data(), v->hw.size()))) return r;
     if ((r = m.upload(&v->d_tiles, v->tiles.data(), v->tiles.size()))) return r;
-    if ((r = m.upload(&v->d_case_tile_start, v->case_tile_start.data(), v->case_tile_start.size()))) return r;
+    if ((r = m.upload(&v->d_case_slot_start, v->case_slot_start.data(), v->case_slot_start.size()))) return r;
     if ((r = m.upload(&v->d_seg_rhs, v->seg_rhs.data(), v->seg_rhs.size()))) return r;
     if ((r = m.upload(&v->d_seg_all, v->seg_all.data(), v->seg_all.size()))) return r;
-    if ((r = m.alloc(&v->cmf_part, v->tiles.size()))) return r;
+    if ((r = m.alloc(&v->cmf_part, (size_t)v->cmf_slot_start.back()))) return r;
     if ((r = m.alloc(&v->cmf_delta, (size_t)n))) return r;
     CK(cudaMemset(v->cmf_delta, 0, sizeof(double) * n));
     if ((r = m.alloc(&v->dt_part, (size_t)v->cta_start.back()))) return r;
@@ -404,7 +417,7 @@ int run_stage(View* v, Prof* pf, int stage, double* const* q_in, const double* c
     A.tiles = v->d_tiles; A.ntiles = (int)v->tiles.size();
     A.stage = stage;
     A.ncases = v->ncases;
-    A.case_tile_start = v->d_case_tile_start;
+    A.case_slot_start = v->d_case_slot_start;
     A.cmf_part = (stage == 3 && v->any_cmf) ? v->cmf_part : nullptr;
     A.cmf_counter = v->counters + 1;
     A.cmf_delta = v->cmf_delta;
@@ -414,6 +427,7 @@ int run_stage(View* v, Prof* pf, int stage, double* const* q_in, const double* c
         A.p[b].q0 = q0 ? q0[b] : q_in[b];
         A.p[b].q_out = q_out[b];
         A.p[b].spmean = spm[b];
+        A.cmf_slot_start[b] = v->cmf_slot_start[b];
     }
     LaunchScope ls(pf, WM_KIND_STAGE, s);
     CK(launch_stage(A, v->opts, s));
@@ -584,10 +598,7 @@ int wm_case_create(const wm_case_desc* d, wm_case** out) {
         }
     }
 
-    // ---- stage tiles (fixed per case: results do not depend on batch membership)
-    int tj, tk;
-    tile_shape(c->opts.tile, &tj, &tk);
-    build_tiles(c, tj, tk, choose_chunk(c->hb, c->opts, tj, tk, d->chunk));
+    c->chunk_req = d->chunk > 0 ? d->chunk : 0;
 
     c->self = new View();
     wm_case* self_list[1] = {c};

@@ -372,7 +372,16 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
 
     const int i0 = t.i0, i1 = t.i1;
     const double dt = A.stage ? *A.dt[B.case_id] : 0.0;
+    // constant mass flux (stage 3): one partial of rho u_dir V per (tile column, plane, warp),
+    // so the case's sum does not depend on how the columns are cut into chunks along i
+    const bool cmf_on = A.stage == 3 && A.cmf_part != nullptr && C.cmf_dir >= 0;
     double cmf_acc = 0.0;
+    double* cmf_col = nullptr;
+    if (cmf_on) {
+        const int ncolk = (B.n[2] + TK - 1) / TK;
+        const int col = ((t.j0 - ng) / TJ) * ncolk + (t.k0 - ng) / TK;
+        cmf_col = A.cmf_part + A.cmf_slot_start[t.blk] + (long long)col * B.n[0] * (NT / 32) + (tid >> 5);
+    }
 
     // ---- RK epilogue of interior cell (io, j, k): r = -(div F)/V (+ source), stage update
     auto output = [&](int io, const R Fhi[5]) {
@@ -457,6 +466,12 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
 #pragma unroll
             for (int v = 0; v < 5; ++v) Flo[v] = Fhi[v];
         }
+        if (cmf_on) {
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) cmf_acc += __shfl_down_sync(0xffffffffu, cmf_acc, off);
+            if ((tid & 31) == 0) cmf_col[(ip - 1 - ng) * (NT / 32)] = cmf_acc;
+            cmf_acc = 0.0;
+        }
         if (ip < i1)
             for (int f = tid; f < LY::FJN + LY::FKN; f += NT) jk_face(ip, f);
         cp_async_wait_all();
@@ -468,37 +483,30 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
     }
 
     if (A.stage == 3 && A.cmf_part != nullptr) {
-        // fixed-order block reduction -> one partial per tile
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) cmf_acc += __shfl_down_sync(0xffffffffu, cmf_acc, off);
-        if ((tid & 31) == 0) red[tid >> 5] = cmf_acc;
-        __syncthreads();
+        // every CTA of the launch signals; the last one reduces each case's partials
         __shared__ bool last;
-        if (tid == 0) {
-            double s = 0.0;
-            for (int w = 0; w < NT / 32; ++w) s += red[w];
-            A.cmf_part[blockIdx.x] = s;
-            __threadfence();
-            last = atomicAdd(A.cmf_counter, 1u) == unsigned(gridDim.x - 1);
-        }
+        if (cmf_on && (tid & 31) == 0) __threadfence();
+        __syncthreads();
+        if (tid == 0) last = atomicAdd(A.cmf_counter, 1u) == unsigned(gridDim.x - 1);
         __syncthreads();
         if (last) {
-            // the last tile sums each case's partials over that case's tiles in a fixed order
-            // (the same alone or in a batch, run to run) and forms its shift
+            // per case: the sum over that case's partials in slot order (the same alone or in
+            // a batch, for any chunk length, run to run) and the shift
             // delta = target - sum(rho u V) / sum(V), wmles/solver.py:24-29
             __threadfence();
             const volatile double* part = A.cmf_part;
             for (int c = 0; c < A.ncases; ++c) {
                 const CaseDev& Cc = A.cases[c];
-                const int t0 = A.case_tile_start[c], t1 = A.case_tile_start[c + 1];
+                if (Cc.cmf_dir < 0) continue;
+                const int s0 = A.case_slot_start[c], s1 = A.case_slot_start[c + 1];
                 double s = 0.0;
-                for (int i = t0 + tid; i < t1; i += NT) s += part[i];
+                for (int i = s0 + tid; i < s1; i += NT) s += part[i];
 #pragma unroll
                 for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
                 __syncthreads();
                 if ((tid & 31) == 0) red[tid >> 5] = s;
                 __syncthreads();
-                if (tid == 0 && Cc.cmf_dir >= 0) {
+                if (tid == 0) {
                     double tot = 0.0;
                     for (int w = 0; w < NT / 32; ++w) tot += red[w];
                     A.cmf_delta[c] = Cc.cmf_target - tot / Cc.cmf_volume;

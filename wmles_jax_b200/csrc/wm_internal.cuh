@@ -87,11 +87,12 @@ struct StageArgs {
     int ntiles;
     int stage;                    // 0: q_out = RHS; 1,2,3: SSP-RK3 stage
     int ncases;
-    const int* case_tile_start;   // ncases + 1: tiles of case c are [start[c], start[c+1])
-    double* cmf_part;             // stage 3 with constant mass flux: per-tile partial sums
+    const int* case_slot_start;   // ncases + 1: partial-sum slots of case c are [start[c], start[c+1])
+    double* cmf_part;             // stage 3 with constant mass flux: per (column, plane, warp) partials
     unsigned int* cmf_counter;    // last-CTA-done counter (the last CTA resets it)
     double* cmf_delta;            // per case: constant-mass-flux shift, written by the last CTA
     const double* dt[MAX_CASES];  // per case: device time step
+    int cmf_slot_start[WM_MAX_BLOCKS];   // first partial-sum slot of each block
     StatePtrs p[WM_MAX_BLOCKS];
 };
 

@@ -13,8 +13,12 @@ waiting ones, so requests that arrive while others run join the next step.
 * Admission: a request is admitted when its estimated device bytes fit in the free HBM
   (device free memory plus what PyTorch's allocator holds unused) minus a reserve, and the
   batch has block slots left (at most ``WM_MAX_BLOCKS`` blocks per batch).
-* Host preparation (mesh, metrics, ghost programs, initial state) runs on a builder thread,
-  overlapping the GPU steps; graph captures and case construction exclude each other.
+* Admission order is shortest-job-first (least cells x steps) among arrived requests, or
+  FIFO; a cell budget caps the resident set at a few GPU-fulls of cells, so short requests
+  do not wait behind long ones while the GPU stays full.
+* Host preparation (lowering, ghost programs, initial state) runs on builder threads,
+  overlapping the GPU steps; graph captures and device-side case construction exclude each
+  other.
 * Results do not depend on the mix: per-case reductions run over that case's own cells in
   a fixed order and its stage tiles are fixed at construction, so a case advanced in any
   batch is bit-identical to the same case advanced alone with ``Solver.step``.
@@ -116,34 +120,63 @@ def free_device_bytes(device=None):
 
 
 class Admission:
-    """Admission bookkeeping: bytes reserved by admitted-but-unbuilt or resident cases are
-    charged against a budget measured once at start (device free bytes minus a reserve), so
-    decisions do not race with allocations in flight."""
+    """Admission bookkeeping.  Bytes, blocks and interior cells of admitted cases (resident,
+    or admitted and still being built) are charged against limits fixed at start: a byte
+    budget (device free bytes minus a reserve), the batch's block slots, and a cell budget
+    that keeps one batch step large enough to fill the GPU without making every resident
+    case wait for all the others (None: no cell limit).  A case is always admitted into an
+    empty server if its bytes fit."""
 
-    def __init__(self, budget_bytes, max_blocks=N.MAX_BLOCKS, max_cases=N.MAX_BLOCKS):
+    def __init__(self, budget_bytes, max_blocks=N.MAX_BLOCKS, max_cases=N.MAX_BLOCKS, max_cells=None):
         self.budget, self.max_blocks, self.max_cases = int(budget_bytes), max_blocks, max_cases
+        self.max_cells = max_cells
         self.used = 0
         self.blocks = 0
         self.cases = 0
+        self.cells = 0
         self.peak = 0             # most bytes ever charged at once
 
-    def fits(self, nbytes, nblocks):
+    def fits(self, nbytes, nblocks, ncells=0):
         if nbytes > self.budget or nblocks > self.max_blocks:
             raise ValueError(f"request needs {nbytes} bytes / {nblocks} blocks: it can never be admitted "
                              f"(budget {self.budget} bytes, {self.max_blocks} blocks)")
+        cells_ok = self.max_cells is None or self.cases == 0 or self.cells + ncells <= self.max_cells
         return (self.used + nbytes <= self.budget and self.blocks + nblocks <= self.max_blocks
-                and self.cases + 1 <= self.max_cases)
+                and self.cases + 1 <= self.max_cases and cells_ok)
 
-    def take(self, nbytes, nblocks):
+    def take(self, nbytes, nblocks, ncells=0):
         self.used += nbytes
         self.peak = max(self.peak, self.used)
         self.blocks += nblocks
         self.cases += 1
+        self.cells += ncells
 
-    def give(self, nbytes, nblocks):
+    def give(self, nbytes, nblocks, ncells=0):
         self.used -= nbytes
         self.blocks -= nblocks
         self.cases -= 1
+        self.cells -= ncells
+
+
+def order_key(policy):
+    """Admission order among arrived requests: "sjf" = least work (cells x steps) first, ties
+    by arrival; "fifo" = arrival order."""
+    if policy == "sjf":
+        return lambda r: (r.cells * r.steps, r.arrival, r.rid)
+    if policy == "fifo":
+        return lambda r: (r.arrival, r.rid)
+    raise ValueError(f"unknown admission policy {policy!r}")
+
+
+def pick_next(waiting, admission, precision, policy):
+    """The first arrived request, in policy order, that the admission limits accept (None if
+    none fits now).  Under "fifo" a request that does not fit blocks the ones behind it."""
+    for r in sorted(waiting, key=order_key(policy)):
+        if admission.fits(estimate_bytes(r.dims, precision), len(r.dims), r.cells):
+            return r
+        if policy == "fifo":
+            return None
+    return None
 
 
 @dataclass
@@ -178,18 +211,25 @@ class Result:
 class Server:
     """Continuous-batching server (see the module docstring).
 
-    precision / tile / chunk: solver options shared by every case (one batch); graphs: replay
+    precision / tile / chunk: solver options shared by every case (one batch; tile="auto" tunes
+    the tile shape over the grids of the requests before serving); graphs: replay
     steps from CUDA graphs once a membership has run ``graph_after`` steps eagerly;
-    reserve_bytes: HBM left free; budget_bytes: override of the admission budget."""
+    reserve_bytes: HBM left free; budget_bytes: override of the admission budget; max_cells:
+    interior-cell budget of the resident set; policy: admission order ("sjf" or "fifo");
+    builders: host threads preparing admitted cases."""
 
     def __init__(self, precision="mixed", tile=None, chunk=None, graphs=True, graph_after=2,
-                 reserve_bytes=4 << 30, budget_bytes=None, device=None):
+                 reserve_bytes=4 << 30, budget_bytes=None, max_cells=8 << 20, policy="sjf", builders=2,
+                 device=None):
         from .backend import require_gpu
         self.device = device or require_gpu()
         self.precision, self.tile, self.chunk = precision, tile, chunk
+        self.tuned = None
         self.graphs, self.graph_after = graphs, graph_after
+        order_key(policy)
+        self.policy, self.builders = policy, max(1, int(builders))
         budget = budget_bytes if budget_bytes is not None else free_device_bytes(self.device) - reserve_bytes
-        self.admission = Admission(max(0, budget))
+        self.admission = Admission(max(0, budget), max_cells=max_cells)
         self.stream = torch.cuda.Stream(self.device)
         self._lock = threading.Lock()             # case construction vs graph capture
         self._cond = threading.Condition()        # admission waits for retirements
@@ -197,40 +237,67 @@ class Server:
 
     # ------------------------------------------------------------------ building
     def _build(self, req, bstream):
+        """Host work (lowering, initial state) unlocked; device work under the lock that keeps
+        it out of graph captures."""
         from .solver import Solver
         mesh, gas, kw, prim = req.build()
-        for src in kw.get("sources", ()):
-            if hasattr(src, "fill_at_time"):
-                raise NotImplementedError("the server advances time-independent cases only")
+        solver = Solver.__new__(Solver)
+        solver._prepare(mesh, gas, precision=self.precision, tile=self.tile, chunk=self.chunk, **kw)
+        if solver.has_inflow:
+            raise NotImplementedError("the server advances cases without a synthetic inflow only")
+        # the initial state exactly as Solver.init_state builds it
+        q0 = [np.ascontiguousarray(gas.prim_to_cons(np.asarray(prim(g.xc), float))) for g in solver.geoms]
         with self._lock, torch.cuda.stream(bstream):
-            solver = Solver(mesh, gas, precision=self.precision, tile=self.tile, chunk=self.chunk, **kw)
-            if solver.has_inflow:
-                raise NotImplementedError("the server advances cases without a synthetic inflow only")
-            qa = solver.init_state(prim)
+            solver._create()
+            qa = tuple(torch.from_numpy(q).to(self.device) for q in q0)
             qb = tuple(torch.empty_like(q) for q in qa)
             da = solver.max_dt(qa)
             db = torch.empty_like(da)
             bstream.synchronize()
         return solver, [qa, qb], [da, db]
 
-    def _builder(self, requests, t0, ready, errors):
+    def _builder(self, todo, t0, ready, errors, left):
         bstream = torch.cuda.Stream(self.device)
         try:
-            for req in requests:
-                delay = t0 + req.arrival - time.perf_counter()
-                if delay > 0:
-                    time.sleep(delay)
-                nbytes = estimate_bytes(req.dims, self.precision)
+            while True:
                 with self._cond:
-                    while not self.admission.fits(nbytes, len(req.dims)):
-                        self._cond.wait(timeout=0.05)
-                    self.admission.take(nbytes, len(req.dims))
+                    while True:
+                        if errors:
+                            return
+                        if not todo:
+                            return
+                        now = time.perf_counter() - t0
+                        waiting = [r for r in todo if r.arrival <= now]
+                        req = pick_next(waiting, self.admission, self.precision, self.policy)
+                        if req is not None:
+                            break
+                        nxt = min(r.arrival for r in todo) - now
+                        self._cond.wait(timeout=min(0.05, nxt) if nxt > 0 else 0.05)
+                    todo.remove(req)
+                    nbytes = estimate_bytes(req.dims, self.precision)
+                    self.admission.take(nbytes, len(req.dims), req.cells)
                 solver, bufs, dts = self._build(req, bstream)
                 ready.put(_Resident(req, solver, bufs, dts, nbytes, admitted=time.perf_counter() - t0))
         except BaseException as e:   # surfaced by run()
             errors.append(e)
         finally:
-            ready.put(None)
+            with self._cond:
+                left[0] -= 1
+                last = left[0] == 0
+                self._cond.notify_all()
+            if last:
+                ready.put(None)
+
+    def tune(self, requests):
+        """Tile shape for this server's cases: one case of each distinct grid of ``requests``,
+        advanced together under each candidate tile (autotune.tune, cached)."""
+        from .autotune import tune
+        seen, cases = set(), []
+        for r in requests:
+            if r.dims not in seen:
+                seen.add(r.dims)
+                cases.append(r.build())
+        return tune(cases, precision=self.precision)
 
     # ------------------------------------------------------------------ stepping
     def _capture(self, batch, args):
@@ -240,24 +307,43 @@ class Server:
             return None
         try:
             g = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(g, stream=self.stream, capture_error_mode="thread_local"):
-                batch.step_args(args, self.stream)
+            with torch.cuda.stream(self.stream):
+                g.capture_begin(capture_error_mode="thread_local")
+                try:
+                    batch.step_args(args, self.stream)
+                finally:
+                    g.capture_end()
             return g
         finally:
             self._lock.release()
 
     def run(self, requests, timeout=None):
         """Serve ``requests`` (arrival times relative to now); returns {rid: Result}."""
-        requests = sorted(requests, key=lambda r: r.arrival)
-        ready, errors = queue.Queue(), []
+        if self.tile == "auto":
+            self.tuned = self.tune(requests)
+            self.tile = self.tuned[0]
+        todo = sorted(requests, key=lambda r: r.arrival)
+        ready, errors, left = queue.Queue(), [], [self.builders]
         t0 = time.perf_counter()
-        builder = threading.Thread(target=self._builder, args=(requests, t0, ready, errors), daemon=True)
-        builder.start()
+        workers = [threading.Thread(target=self._builder, args=(todo, t0, ready, errors, left), daemon=True)
+                   for _ in range(self.builders)]
+        for w in workers:
+            w.start()
         active, joined, results = [], [], {}
         pending = []               # (event, [residents finished by that step]) of steps in flight
         batch, args, graphs, run_len = None, {}, {}, 0
         builder_done = False
         n = dict(batch_steps=0, graph_steps=0, captures=0, memberships=0, kernel_launches=0, cell_steps=0)
+        seg, busy_ms = None, 0.0    # device time of the batch steps, per membership segment
+
+        def close_segment():
+            nonlocal seg, busy_ms
+            if seg is not None:
+                end = torch.cuda.Event(enable_timing=True)
+                end.record(self.stream)
+                end.synchronize()
+                busy_ms += seg.elapsed_time(end)
+                seg = None
 
         def clock():
             return time.perf_counter() - t0
@@ -284,7 +370,7 @@ class Server:
                     r.bufs[1 - r.parity] = None
                     r.dts[1 - r.parity] = None
                     r.solver = None
-                    self.admission.give(r.nbytes, len(r.req.dims))
+                    self.admission.give(r.nbytes, len(r.req.dims), r.req.cells)
                 self._cond.notify_all()
 
         with torch.cuda.stream(self.stream):
@@ -306,6 +392,7 @@ class Server:
                 leaving = [r for r in active if r.done >= r.req.steps]
                 if joined or leaving or (batch is None and active):
                     # membership change: drain the steps in flight, free the leavers, rebuild
+                    close_segment()
                     self.stream.synchronize()
                     stamp(0)
                     graphs.clear()
@@ -327,6 +414,8 @@ class Server:
                         batch = Batch([r.solver for r in active])
                         n["memberships"] += 1
                         run_len = 0
+                        seg = torch.cuda.Event(enable_timing=True)
+                        seg.record(self.stream)
                 if not active:
                     if builder_done and ready.empty():
                         break
@@ -362,17 +451,21 @@ class Server:
                 ev.record(self.stream)
                 pending.append((ev, fin))
                 stamp(2)                       # at most two steps in flight
+            close_segment()
             self.stream.synchronize()
             stamp(0)
             if batch is not None:
                 batch.close()
-        builder.join()
+        for w in workers:
+            w.join()
         if errors:
             raise errors[0]
         wall = max((r.finished for r in results.values()), default=0.0)
         ttr = np.array([r.time_to_result for r in results.values()])
         self.stats = dict(n, requests=len(results), wall_s=wall, peak_admitted_bytes=self.admission.peak,
                           mcell_steps_per_s=n["cell_steps"] / wall / 1e6 if wall > 0 else 0.0,
+                          device_busy_s=busy_ms * 1e-3,
+                          device_mcell_steps_per_s=n["cell_steps"] / (busy_ms * 1e-3) / 1e6 if busy_ms > 0 else 0.0,
                           p50_s=float(np.percentile(ttr, 50)) if len(ttr) else None,
                           p99_s=float(np.percentile(ttr, 99)) if len(ttr) else None)
         return results

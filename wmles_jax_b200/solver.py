@@ -44,6 +44,19 @@ def _scheme_fields(scheme):
 class Solver:
     def __init__(self, mesh, gas, scheme, sgs="vreman", cfl=0.8, sgs_kwargs=None, constraints=(),
                  sources=(), bc_passes=2, *, precision="fp64", tile=None, chunk=None):
+        if tile == "auto":           # measured once per workload and machine, then cached
+            from .autotune import tune
+            kw = dict(scheme=scheme, sgs=sgs, cfl=cfl, sgs_kwargs=sgs_kwargs, constraints=constraints,
+                      sources=sources, bc_passes=bc_passes)
+            tile, _ = tune([(mesh, gas, kw, None)], precision=precision)
+        self._prepare(mesh, gas, scheme, sgs, cfl, sgs_kwargs, constraints, sources, bc_passes,
+                      precision=precision, tile=tile, chunk=chunk)
+        self._create()
+
+    def _prepare(self, mesh, gas, scheme, sgs="vreman", cfl=0.8, sgs_kwargs=None, constraints=(),
+                 sources=(), bc_passes=2, *, precision="fp64", tile=None, chunk=None):
+        """Host half of construction: validation and lowering into a case descriptor (no
+        device call; a server runs it on a worker thread)."""
         self.device = require_gpu()
         self.mesh, self.blocks, self.gas = mesh, mesh.blocks, gas
         self.geoms = mesh.geoms
@@ -59,11 +72,16 @@ class Solver:
             raise NotImplementedError(f"cuda backend: more than {N.MAX_BLOCKS} blocks")
         self._lib = N.load()
         self._keep = []
-        desc = self._lower(tile, chunk)
+        self._desc = self._lower(tile, chunk)
+
+    def _create(self, release=True):
+        """Device half of construction: wm_case_create uploads the descriptor's arrays (kept
+        with release=False, e.g. to create the case again with another tile shape)."""
         handle = C.c_void_p()
-        N.check(self._lib.wm_case_create(C.byref(desc), C.byref(handle)), "wm_case_create")
+        N.check(self._lib.wm_case_create(C.byref(self._desc), C.byref(handle)), "wm_case_create")
         self._case = handle
-        self._keep = None         # host arrays were copied to the device
+        if release:
+            self._keep = self._desc = None         # host arrays were copied to the device
 
     def __del__(self):
         h = getattr(self, "_case", None)
