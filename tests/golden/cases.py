@@ -182,50 +182,7 @@ def channel_laminar_prim(gas, seed=0, noise=0.05):
 
 
 # ----------------------------------------------------------------------------- smooth ramp
-RAMP_H, RAMP_TOP, RAMP_SPAN = 0.22, 0.74, 0.288
-
-
-def ramp_props(gas, Ma=0.2, Re_L=667000.0, T_inf=300.0, p_inf=101325.0):
-    rho = p_inf / (gas.R * T_inf)
-    mu = gas.mu_ref * (T_inf / gas.T_ref) ** 1.5 * (gas.T_ref + gas.S_suth) / (T_inf + gas.S_suth)
-    U = Ma * float(np.sqrt(gas.gamma * gas.R * T_inf))
-    L = Re_L * (mu / rho) / U
-    return dict(gas=gas, Ma_inf=Ma, Re_L=Re_L, T_inf=T_inf, p_inf=p_inf, rho_inf=rho,
-                mu_inf=mu, nu_inf=mu / rho, U_inf=U, L=L)
-
-
-def ramp_profile(n=80, delta=0.028, y0=RAMP_H, intensity=0.05):
-    """Analytic inflow table [y/L, U, V, uu, vv, ww, uv] (normalised by U_inf): a 1/7-power
-    boundary layer of thickness ``delta`` with Reynolds stresses peaking near the wall at
-    ``intensity``^2 and vanishing outside the layer."""
-    y = y0 + np.concatenate([np.linspace(0.0, 2 * delta, n - 10), np.linspace(2.2 * delta, 0.6, 10)])
-    eta = np.clip((y - y0) / delta, 0.0, 1.0)
-    U = eta ** (1.0 / 7.0)
-    V = 0.002 * eta
-    shape = np.exp(-((eta - 0.1) / 0.35) ** 2) * (eta < 1.0) + 1e-6
-    uu = (intensity ** 2) * shape * 2.0
-    vv = (intensity ** 2) * shape * 0.6
-    ww = (intensity ** 2) * shape * 1.0
-    uv = -0.4 * np.sqrt(uu * vv)
-    return np.stack([y, U, V, uu, vv, ww, uv], axis=1)
-
-
-def ramp_nodes(n, x_range=(-0.76, 4.0), ratio=1.08, L=1.0):
-    """Structured ramp nodes: quintic ramp wall from y=0.22 (x<=0) to 0 (x>=1), slip top
-    at 0.74, geometric wall-normal stretching ``ratio``, periodic span 0.288 (all / L)."""
-    ni, nj, nk = n
-    x = np.linspace(x_range[0], x_range[1], ni + 1)
-    xi = np.clip(x, 0.0, 1.0)
-    wall = RAMP_H * (1.0 - (10.0 * xi ** 3 - 15.0 * xi ** 4 + 6.0 * xi ** 5))
-    s = np.concatenate([[0.0], np.cumsum(ratio ** np.arange(nj))])
-    s = s / s[-1]
-    y = wall[:, None] + (RAMP_TOP - wall[:, None]) * s[None, :]
-    z = np.linspace(0.0, RAMP_SPAN, nk + 1)
-    shape = (ni + 1, nj + 1, nk + 1)
-    X = np.broadcast_to(x[:, None, None], shape)
-    Y = np.broadcast_to(y[:, :, None], shape)
-    Z = np.broadcast_to(z[None, None, :], shape)
-    return np.stack((X, Y, Z)) * L
+from wmles_jax_b200.workloads import RAMP_H, RAMP_SPAN, RAMP_TOP, ramp_nodes, ramp_profile, ramp_props  # noqa: E402,F401
 
 
 def ramp_case(W, n=(12, 8, 6), scheme_factory=None, sgs="vreman", seed=0, n_modes=16,
@@ -270,9 +227,9 @@ def ramp_prim(props, profile, seed=0):
 # ----------------------------------------------------------------------------- golden table
 SMALL_CASES = ["single_slip_kep4", "split_slip_kep4", "flip_slip_kep4", "rotcyc_slip_kep4",
                "split_wm_hybrid", "flip_wmad_kep2", "single_per_muscl", "rotcyc_per_minmod",
-               "zoo_hybrid", "zoo_kep4", "ramp_small", "channel_small_cmf"]
+               "zoo_hybrid", "zoo_kep4", "ramp_small", "channel_small_cmf", "naca_small"]
 GEOM_CASES = {"single_slip_kep4", "split_slip_kep4", "flip_slip_kep4", "rotcyc_slip_kep4",
-              "zoo_hybrid", "ramp_small"}
+              "zoo_hybrid", "ramp_small", "naca_small"}
 
 
 def golden_case(W, tag):
@@ -299,6 +256,12 @@ def golden_case(W, tag):
     if tag == "ramp_small":
         mesh, gas, props, profile, kw = ramp_case(W)
         return mesh, gas, kw, ramp_prim(props, profile), 0.05 * props["L"] / props["U_inf"]
+    if tag == "naca_small":
+        # the config-4 C-grid with every cell count divided by 8 (four blocks, transposed and
+        # flipped interfaces, wall model on two blocks, far field and outflow)
+        from wmles_jax_b200.workloads import naca_case
+        mesh, gas, kw, prim = naca_case(scale=8, api=W)
+        return mesh, gas, kw, prim, 0.0
     if tag == "channel_small_cmf":
         gas = channel_gas(W)
         mesh = channel_case(W, n=(8, 8, 6), blocks=2)

@@ -17,6 +17,7 @@ import types
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))     # node generators of wmles_jax_b200.workloads (NumPy only)
 
 
 def load_reference(root):
@@ -73,9 +74,11 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
     ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--skip-cfg1", action="store_true", help="keep the existing config-1 fixture")
     args = ap.parse_args()
     W = load_reference(args.reference)
     sys.path.insert(0, HERE)
+    sys.path.append(ROOT)
     import cases as C
 
     # ---------------------------------------------------------------- small topology/physics cases
@@ -115,6 +118,8 @@ def main():
     print("wrote golden_cases.npz:", len(out), "arrays")
 
     # ---------------------------------------------------------------- config-1 channel, 100 steps
+    if args.skip_cfg1:
+        return
     mesh, gas, kw, prim = C.cfg1_case(W)
     solver = W.Solver(mesh, gas, **kw)
     Q = solver.init_state(prim)

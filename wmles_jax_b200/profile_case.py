@@ -1,42 +1,80 @@
-"""Run a few steps of a channel workload on cuda:0 (target for ncu captures).
+"""Run steps of one benchmark configuration on cuda:0 and report its throughput (also the
+target command for ncu captures).
 
-    python -m wmles_jax_b200.profile_case --n 128 128 128 --steps 3 --precision fp64
+    python -m wmles_jax_b200.profile_case --config 2 --n 128 128 128 --steps 3 --precision fp64
+    python -m wmles_jax_b200.profile_case --config 3 --steps 500 --precision mixed
+    python -m wmles_jax_b200.profile_case --config 4 --steps 500 --precision fp64 --breakdown
 
-Builds the config-2 channel physics (KEP4 + WALE + wall model + constant mass flux) at
-the requested size, runs ``--steps`` steps through ``Solver.step`` and prints the wall
-time per step.  Each step launches, in order: dt (1), then per RK stage ghost gather,
-wall model, stage kernel (3 x 3), then the constraint pass (1).
+config 2: periodic channel (KEP4 + WALE + wall model + constant mass flux), size --n;
+config 3: smooth ramp (Hybrid + Vreman + wall model + synthetic inflow + sponge), size --n
+(default 384 96 64); config 4: NACA 0012 four-block C-grid (Hybrid + Vreman + wall model
++ far field), cell counts divided by --scale.  Steps go through ``Solver.step`` with the
+time advanced by the returned dt, as the reference's drivers do.  --breakdown times every
+launch with CUDA events and prints the device time per kernel kind.
 """
 import argparse
+import json
 import time
 
 import numpy as np
 import torch
 
+from . import _native as N
 from .solver import Solver
-from .workloads import channel_case
+from .workloads import channel_case, naca_case, ramp_case
+
+
+def build(config, n=None, scale=1):
+    if config == 2:
+        return channel_case(2, n=tuple(n) if n else (128, 128, 128))
+    if config == 3:
+        mesh, gas, kw, prim, _ = ramp_case(tuple(n) if n else (384, 96, 64))
+        return mesh, gas, kw, prim
+    if config == 4:
+        return naca_case(scale=scale)
+    raise ValueError(f"unknown config {config}")
+
+
+def run(config, precision, steps, n=None, scale=1, tile=None, chunk=None, breakdown=False, warmup=2):
+    mesh, gas, kw, prim = build(config, n, scale)
+    s = Solver(mesh, gas, **kw, precision=precision, tile=tile, chunk=chunk)
+    Q = s.init_state(prim)
+    t = 0.0
+    for _ in range(warmup):
+        Q, dt = s.step(Q, t)
+        t += float(dt)
+    torch.cuda.synchronize()
+    s.profile(enable=breakdown)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        Q, dt = s.step(Q, t)
+        t += float(dt)
+    torch.cuda.synchronize()
+    el = (time.perf_counter() - t0) / steps
+    cells = sum(int(np.prod(b.n)) for b in mesh.blocks)
+    out = {"config": config, "precision": precision, "blocks": [list(b.n) for b in mesh.blocks], "cells": cells,
+           "steps": steps, "ms_per_step": el * 1e3, "mcell_steps_per_s": cells / el / 1e6, "time": t,
+           "finite": all(bool(torch.isfinite(q).all()) for q in Q)}
+    if breakdown:
+        names = {N.KIND_STAGE: "stage", N.KIND_GHOST: "ghost", N.KIND_WALL: "wall", N.KIND_DT: "dt",
+                 N.KIND_SOURCE: "source"}
+        out["device_ms_per_step"] = {names[k]: s.profile_read(k)[0] / steps for k in names}
+        out["launches_per_step"] = s.profile_read(-1)[1] / steps
+    return out
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--n", type=int, nargs=3, default=(128, 128, 128))
+    ap.add_argument("--config", type=int, choices=[2, 3, 4], default=2)
+    ap.add_argument("--n", type=int, nargs=3, default=None)
+    ap.add_argument("--scale", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--tile", type=int, default=None)
     ap.add_argument("--chunk", type=int, default=None)
+    ap.add_argument("--breakdown", action="store_true")
     a = ap.parse_args()
-    mesh, gas, kw, prim = channel_case(2, n=tuple(a.n))
-    s = Solver(mesh, gas, **kw, precision=a.precision, tile=a.tile, chunk=a.chunk)
-    Q = s.init_state(prim)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(a.steps):
-        Q, dt = s.step(Q)
-    torch.cuda.synchronize()
-    el = (time.perf_counter() - t0) / a.steps
-    cells = int(np.prod(a.n))
-    print(f"{a.precision} n={tuple(a.n)}: {el * 1e3:.3f} ms/step (wall), {cells / el / 1e6:.1f} Mcell-steps/s, "
-          f"dt={float(dt):.4e}")
+    print(json.dumps(run(a.config, a.precision, a.steps, a.n, a.scale, a.tile, a.chunk, a.breakdown)), flush=True)
 
 
 if __name__ == "__main__":

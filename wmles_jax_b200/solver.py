@@ -148,7 +148,12 @@ class Solver:
             walls[w].isothermal = 0 if bc.T_wall is None else 1
             walls[w].T_wall = 0.0 if bc.T_wall is None else float(bc.T_wall)
             walls[w].kappa, walls[w].B, walls[w].n_iter = float(m.kappa), float(m.B), int(m.n_iter)
-            walls[w].geom = N.as_double_p(self._arr(wall_geometry(b, self.geoms[ib], a, s, bc.n_match), np.float64))
+            blk = self.blocks[ib]
+            geo = wall_geometry(blk, self.geoms[ib], a, s, bc.n_match)
+            nt = [blk.n[t] for t in range(3) if t != a]
+            if geo.shape != (5, nt[0], nt[1]):
+                raise RuntimeError(f"wall geometry of block {blk.name}: shape {geo.shape}, expected {(5, *nt)}")
+            walls[w].geom = N.as_double_p(self._arr(geo, np.float64))
         self._keep.append(walls)
         d.nwalls, d.walls = len(self.walls), walls
         # ghost programs

@@ -115,6 +115,207 @@ def channel_case(config=2, n=None, blocks=None):
     return mesh, gas, kw, loglaw_prim(gas, mesh)
 
 
+# ---------------------------------------------------------------------------- smooth ramp (config 3)
+RAMP_H, RAMP_TOP, RAMP_SPAN = 0.22, 0.74, 0.288
+
+
+def ramp_props(gas, Ma=0.2, Re_L=667000.0, T_inf=300.0, p_inf=101325.0):
+    rho = p_inf / (gas.R * T_inf)
+    mu = gas.mu_ref * (T_inf / gas.T_ref) ** 1.5 * (gas.T_ref + gas.S_suth) / (T_inf + gas.S_suth)
+    U = Ma * float(np.sqrt(gas.gamma * gas.R * T_inf))
+    L = Re_L * (mu / rho) / U
+    return dict(gas=gas, Ma_inf=Ma, Re_L=Re_L, T_inf=T_inf, p_inf=p_inf, rho_inf=rho,
+                mu_inf=mu, nu_inf=mu / rho, U_inf=U, L=L)
+
+
+def ramp_profile(n=80, delta=0.028, y0=RAMP_H, intensity=0.05):
+    """Analytic inflow table [y/L, U, V, uu, vv, ww, uv] (normalised by U_inf): a 1/7-power
+    boundary layer of thickness ``delta`` with Reynolds stresses peaking near the wall at
+    ``intensity``^2 and vanishing outside the layer."""
+    y = y0 + np.concatenate([np.linspace(0.0, 2 * delta, n - 10), np.linspace(2.2 * delta, 0.6, 10)])
+    eta = np.clip((y - y0) / delta, 0.0, 1.0)
+    U = eta ** (1.0 / 7.0)
+    V = 0.002 * eta
+    shape = np.exp(-((eta - 0.1) / 0.35) ** 2) * (eta < 1.0) + 1e-6
+    uu = (intensity ** 2) * shape * 2.0
+    vv = (intensity ** 2) * shape * 0.6
+    ww = (intensity ** 2) * shape * 1.0
+    uv = -0.4 * np.sqrt(uu * vv)
+    return np.stack([y, U, V, uu, vv, ww, uv], axis=1)
+
+
+def ramp_nodes(n, x_range=(-0.76, 4.0), ratio=1.08, L=1.0):
+    """Structured ramp nodes: quintic ramp wall from y=0.22 (x<=0) to 0 (x>=1), slip top
+    at 0.74, geometric wall-normal stretching ``ratio``, periodic span 0.288 (all / L)."""
+    ni, nj, nk = n
+    x = np.linspace(x_range[0], x_range[1], ni + 1)
+    xi = np.clip(x, 0.0, 1.0)
+    wall = RAMP_H * (1.0 - (10.0 * xi ** 3 - 15.0 * xi ** 4 + 6.0 * xi ** 5))
+    s = np.concatenate([[0.0], np.cumsum(ratio ** np.arange(nj))])
+    s = s / s[-1]
+    y = wall[:, None] + (RAMP_TOP - wall[:, None]) * s[None, :]
+    z = np.linspace(0.0, RAMP_SPAN, nk + 1)
+    shape = (ni + 1, nj + 1, nk + 1)
+    X = np.broadcast_to(x[:, None, None], shape)
+    Y = np.broadcast_to(y[:, :, None], shape)
+    Z = np.broadcast_to(z[None, None, :], shape)
+    return np.stack((X, Y, Z)) * L
+
+
+def ramp_case(n=(384, 96, 64), n_modes=64, seed=0, sponge_start_l=3.0, x_range=(-0.76, 4.0)):
+    """(mesh, gas, solver kwargs, prim_fn, props) of the smooth-ramp configuration (config 3
+    at the default size): quintic ramp wall with the equilibrium wall model (adiabatic,
+    sampled at the first cell), slip top at y = 0.74 L, periodic span 0.288 L, geometric
+    wall-normal ratio 1.08, Ma_inf 0.2, Re_L 667000; Fourier-mode synthetic inflow with 5 %
+    intensity and scales (0.1, 0.02, 0.03) L on i-min, characteristic outflow on i-max, a
+    spanwise-mean sponge over the last 1 L; Hybrid Ducros KEP4 / MUSCL-HLLC, Vreman.  The
+    inflow profile is the analytic boundary-layer table of ``ramp_profile``."""
+    from .bc import CharacteristicFarfield, SlipWall
+    from .schemes import Hybrid
+    from .smooth_ramp import SmoothRampInflow, SmoothRampSponge
+    gas = Gas()
+    props = ramp_props(gas)
+    profile = ramp_profile()
+    L = props["L"]
+    blk = Block("ramp", ramp_nodes(n, x_range=x_range, L=L))
+    mesh = Mesh([blk])
+    mesh.connect(blk, "kmin", blk, "kmax", shift=(0.0, 0.0, -RAMP_SPAN * L))
+    prim_inf = np.array([props["rho_inf"], props["U_inf"], 0.0, 0.0, props["p_inf"]])
+    blk.set_bc("imin", SmoothRampInflow(props, profile, (0.1, 0.02, 0.03), seed, n_modes, n[2]))
+    blk.set_bc("imax", CharacteristicFarfield(prim_inf))
+    blk.set_bc("jmin", WallModel(EquilibriumWallModel(), T_wall=None, n_match=1))
+    blk.set_bc("jmax", SlipWall())
+    mesh.finalize()
+    sponge = SmoothRampSponge(props, sponge_start_l, x_range[1], 1.0)
+    kw = dict(scheme=Hybrid(KEP(4)), sgs="vreman", cfl=0.5, sources=(sponge,))
+    rng = np.random.default_rng(seed)
+
+    def prim(xc):
+        x, y, _ = xc
+        xi = np.clip(x / L, 0.0, 1.0)
+        wall = RAMP_H * (1.0 - (10.0 * xi ** 3 - 15.0 * xi ** 4 + 6.0 * xi ** 5))
+        yd = y / L - wall + RAMP_H
+        U = props["U_inf"] * np.interp(yd, profile[:, 0], profile[:, 1])
+        pert = rng.normal(0.0, 0.02 * props["U_inf"], size=(3,) + x.shape)
+        one = np.ones_like(x)
+        return np.stack([props["rho_inf"] * one, U + pert[0], pert[1], pert[2], props["p_inf"] * one])
+    return mesh, gas, kw, prim, props
+
+
+# ---------------------------------------------------------------------------- NACA 0012 C-grid (config 4)
+NACA_SPAN, NACA_FAR = 0.0481, 20.0
+
+
+def naca0012_half_thickness(x):
+    """Half thickness of the NACA 0012 section, chord 1: the 4-digit thickness formula with
+    the closed-trailing-edge x^4 coefficient (-0.1036)."""
+    return 0.6 * (0.2969 * np.sqrt(x) - 0.1260 * x - 0.3516 * x ** 2 + 0.2843 * x ** 3 - 0.1036 * x ** 4)
+
+
+def geometric_spacing(n, first, total):
+    """n+1 increasing coordinates from 0 to `total` whose intervals grow by a constant ratio
+    from `first` (uniform when `first` is already the mean interval)."""
+    if first * n >= total:
+        return np.linspace(0.0, total, n + 1)
+    lo, hi = 1.0 + 1e-12, 4.0
+    for _ in range(200):
+        r = 0.5 * (lo + hi)
+        if first * (r ** n - 1.0) / (r - 1.0) < total:
+            lo = r
+        else:
+            hi = r
+    x = np.concatenate([[0.0], np.cumsum(first * (0.5 * (lo + hi)) ** np.arange(n))])
+    return x * (total / x[-1])
+
+
+def naca_cgrid_nodes(scale=1, far=NACA_FAR, span=NACA_SPAN, wall_spacing=2e-3):
+    """Nodes (3, ni+1, nj+1, nk+1) of a four-block C-grid around the NACA 0012 section.
+
+    One algebraic C-mesh: its inner line runs along the lower wake cut (x = far -> 1), around
+    the section (lower surface, leading edge, upper surface; cosine spacing) and along the
+    upper wake cut (1 -> far); its outer line is y = -far, a half circle of radius `far`
+    about the trailing edge, and y = +far; nodes lie on straight lines between the two with
+    geometric wall-normal spacing (first interval ~ wall_spacing).  It is cut into blocks
+    of (at scale 1) 128 x 64 (lower wake, i and j reversed), 256 x 64 (section, trailing
+    edge lower -> leading edge -> upper surface at x ~ 0.65), 64 x 64 (rest of the upper
+    surface, with i and j transposed so its wall is an i face) and 128 x 64 (upper wake);
+    40 spanwise cells over `span`.  `scale` divides every cell count."""
+    n_wake, n_af, n_aft, nj, nk = 128 // scale, 320 // scale, 64 // scale, 64 // scale, 40 // scale
+    s = np.linspace(0.0, 1.0, n_af + 1)
+    xa = 0.5 * (1.0 + np.cos(2.0 * np.pi * s))                      # 1 -> 0 -> 1
+    ya = np.where(s <= 0.5, -1.0, 1.0) * naca0012_half_thickness(xa)
+    xw = 1.0 + geometric_spacing(n_wake, 1.0 - xa[1], far - 1.0)     # 1 -> far
+    phi = -0.5 * np.pi - np.pi * s
+    inner = np.stack([np.concatenate([xw[::-1], xa[1:-1], xw]), np.concatenate([0 * xw, ya[1:-1], 0 * xw])])
+    outer = np.stack([np.concatenate([xw[::-1], 1.0 + far * np.cos(phi[1:-1]), xw]),
+                      np.concatenate([-far + 0 * xw, far * np.sin(phi[1:-1]), far + 0 * xw])])
+    sig = geometric_spacing(nj, wall_spacing / far, 1.0)
+    xy = inner[:, :, None] + sig[None, None, :] * (outer - inner)[:, :, None]      # (2, NI+1, nj+1)
+    z = np.linspace(0.0, span, nk + 1)
+    shp = xy.shape[1:] + (nk + 1,)
+    C = np.stack([np.broadcast_to(xy[0][:, :, None], shp), np.broadcast_to(xy[1][:, :, None], shp),
+                  np.broadcast_to(z[None, None, :], shp)])
+    a0, a1, a2 = n_wake, n_wake + n_af - n_aft, n_wake + n_af
+    return {
+        "wake_lower": np.ascontiguousarray(C[:, a0::-1, ::-1]),
+        "section": np.ascontiguousarray(C[:, a0:a1 + 1]),
+        "section_aft": np.ascontiguousarray(C[:, a1:a2 + 1][:, ::-1].transpose(0, 2, 1, 3)),
+        "wake_upper": np.ascontiguousarray(C[:, a2:]),
+    }
+
+
+def _classes(api):
+    """The public classes a builder needs: `api` (any namespace with the reference's class
+    names, e.g. to feed the same case to another implementation) or this package's."""
+    if api is not None:
+        return api
+    import types
+    from .bc import CharacteristicFarfield
+    from .schemes import Hybrid
+    return types.SimpleNamespace(Gas=Gas, Block=Block, Mesh=Mesh, WallModel=WallModel, KEP=KEP, Hybrid=Hybrid,
+                                 EquilibriumWallModel=EquilibriumWallModel,
+                                 CharacteristicFarfield=CharacteristicFarfield)
+
+
+def naca_case(scale=1, alpha_deg=4.0, Ma=0.15, Re_c=1e6, noise=0.01, seed=0, n_match=3, api=None):
+    """(mesh, gas, solver kwargs, prim_fn) of the NACA 0012 C-grid (config 4 at scale 1):
+    nondimensional gas (rho = T = 1 gives |U| = 1 at Ma, Re on the chord), angle of attack
+    `alpha_deg`, adiabatic equilibrium wall model on the section, characteristic far field
+    and outflow, periodic span; Hybrid Ducros KEP4 / MUSCL-HLLC with Vreman; uniform free
+    stream plus N(0, noise) in u, v, w."""
+    W = _classes(api)
+    Block, Mesh, WallModel, EquilibriumWallModel = W.Block, W.Mesh, W.WallModel, W.EquilibriumWallModel
+    CharacteristicFarfield, Hybrid, KEP = W.CharacteristicFarfield, W.Hybrid, W.KEP
+    nodes = naca_cgrid_nodes(scale)
+    gas = W.Gas(gamma=1.4, R=1.0 / (1.4 * Ma ** 2), mu_ref=1.0 / Re_c, T_ref=1.0, S_suth=110.4 / 300.0)
+    blk = {name: Block(name, x) for name, x in nodes.items()}
+    mesh = Mesh(list(blk.values()))
+    wl, sec, aft, wu = blk["wake_lower"], blk["section"], blk["section_aft"], blk["wake_upper"]
+    mesh.connect(wl, "imin", sec, "imin")          # trailing edge, lower side: i and j reversed
+    mesh.connect(sec, "imax", aft, "jmax")         # upper surface: transposed
+    mesh.connect(aft, "jmin", wu, "imin")          # trailing edge, upper side
+    mesh.connect(wl, "jmax", wu, "jmin")           # wake cut
+    for b in blk.values():
+        mesh.connect(b, "kmin", b, "kmax", shift=(0.0, 0.0, -NACA_SPAN))
+    a = np.deg2rad(alpha_deg)
+    prim_inf = np.array([1.0, np.cos(a), np.sin(a), 0.0, gas.R])
+    m = min(n_match, min(b.n[1] for b in blk.values()))
+    wm = EquilibriumWallModel()
+    sec.set_bc("jmin", WallModel(wm, T_wall=None, n_match=m))
+    aft.set_bc("imin", WallModel(wm, T_wall=None, n_match=m))
+    for b, f in ((sec, "jmax"), (wl, "jmin"), (wl, "imax"), (wu, "jmax"), (wu, "imax"), (aft, "imax")):
+        b.set_bc(f, CharacteristicFarfield(prim_inf))
+    mesh.finalize()
+    kw = dict(scheme=Hybrid(KEP(4)), sgs="vreman", cfl=0.5)
+    rng = np.random.default_rng(seed)
+
+    def prim(xc):
+        one = np.ones_like(xc[0])
+        pert = rng.normal(0.0, noise, size=(3,) + one.shape)
+        return np.stack([one, np.cos(a) + pert[0], np.sin(a) + pert[1], pert[2], gas.R * one])
+    return mesh, gas, kw, prim
+
+
 # algorithmic HBM bytes per interior cell (FP64 / mixed metrics), per stage-kernel launch
 # stage 1: Q read + Q1 write + metrics; stages 2, 3: + Q0 read; CFL/constraint pass: Q + S, V
 STAGE_BYTES = {"fp64": (184, 224, 224), "mixed": (132, 172, 172)}
