@@ -237,12 +237,39 @@ def run_ours(args, rank, world, local_rank):
     }
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.cpu_cells)
-    if world == 1 and args.serving_requests > 0:
+    if world == 1 and args.extra:
         del s64, s32, Q64, Q32, Qn, dbuf
+        line["mixed"]["error_vs_fp64"] = precision_leg()
+        line["configs"] = configs_leg()
+    if world == 1 and args.serving_requests > 0:
         line["serving"] = serving_leg(args)
     if dist is not None:
         dist.destroy_process_group()
     return line
+
+
+# ----------------------------------------------------------------------------- configs 3 and 4, precision
+def configs_leg(steps=100):
+    """Throughput of the smooth ramp (config 3) and the NACA 0012 C-grid (config 4), both forms,
+    tile shape from the autotuner; inputs larger than L2."""
+    from wmles_jax_b200.profile_case import run
+    out = {}
+    for cfg, name in ((3, "smooth ramp 384x96x64, Hybrid + Vreman + wall model + inflow + sponge"),
+                      (4, "NACA 0012 C-grid 4 blocks (576x64x40), Hybrid + Vreman + wall model + far field")):
+        r = {p: run(cfg, p, steps, tile="auto", warmup=3) for p in ("fp64", "mixed")}
+        out[f"config{cfg}"] = {"workload": name, "cells": r["fp64"]["cells"], "steps": steps,
+                               "fp64": r["fp64"]["mcell_steps_per_s"], "mixed": r["mixed"]["mcell_steps_per_s"],
+                               "unit": METRIC, "speedup": r["mixed"]["mcell_steps_per_s"] / r["fp64"]["mcell_steps_per_s"],
+                               "finite": r["fp64"]["finite"] and r["mixed"]["finite"],
+                               "timing": "host clock around steps (the time advances by the returned dt each step)"}
+    return out
+
+
+def precision_leg():
+    """Mixed vs FP64 on config 2 after 1000 steps from the same input, beside two FP64 runs whose
+    inputs differ by a relative 1e-7 (the flow's own sensitivity at that step count)."""
+    from wmles_jax_b200.precision_study import compare
+    return compare(2, 1000, perturb=1e-7)
 
 
 # ----------------------------------------------------------------------------- serving (config 5)
@@ -343,6 +370,8 @@ def main():
     ap.add_argument("--cpu-cells", type=int, default=8, help="x-cells of the CPU slab sample")
     ap.add_argument("--max-workers", type=int, default=64)
     ap.add_argument("--serving-requests", type=int, default=64, help="config-5 requests (0: skip the leg)")
+    ap.add_argument("--no-extra", dest="extra", action="store_false",
+                    help="skip the config-3/4 throughput and the 1000-step precision study")
     ap.add_argument("--serving-steps", type=int, default=2000)
     ap.add_argument("--serving-rate", type=float, default=20.0)
     args = ap.parse_args()

@@ -5,7 +5,8 @@ target command for ncu captures).
     python -m wmles_jax_b200.profile_case --config 3 --steps 500 --precision mixed
     python -m wmles_jax_b200.profile_case --config 4 --steps 500 --precision fp64 --breakdown
 
-config 2: periodic channel (KEP4 + WALE + wall model + constant mass flux), size --n;
+config 2: periodic channel (KEP4 + WALE + wall model + constant mass flux), size --n
+(default 256 128 128);
 config 3: smooth ramp (Hybrid + Vreman + wall model + synthetic inflow + sponge), size --n
 (default 384 96 64); config 4: NACA 0012 four-block C-grid (Hybrid + Vreman + wall model
 + far field), cell counts divided by --scale.  Steps go through ``Solver.step`` with the
@@ -26,7 +27,7 @@ from .workloads import channel_case, naca_case, ramp_case
 
 def build(config, n=None, scale=1):
     if config == 2:
-        return channel_case(2, n=tuple(n) if n else (128, 128, 128))
+        return channel_case(2, n=tuple(n) if n else (256, 128, 128))
     if config == 3:
         mesh, gas, kw, prim, _ = ramp_case(tuple(n) if n else (384, 96, 64))
         return mesh, gas, kw, prim
@@ -70,11 +71,12 @@ def main():
     ap.add_argument("--scale", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
-    ap.add_argument("--tile", type=int, default=None)
+    ap.add_argument("--tile", default=None, help="tile id 0-3 or 'auto' (autotuned, cached)")
     ap.add_argument("--chunk", type=int, default=None)
     ap.add_argument("--breakdown", action="store_true")
     a = ap.parse_args()
-    print(json.dumps(run(a.config, a.precision, a.steps, a.n, a.scale, a.tile, a.chunk, a.breakdown)), flush=True)
+    tile = a.tile if a.tile in (None, "auto") else int(a.tile)
+    print(json.dumps(run(a.config, a.precision, a.steps, a.n, a.scale, tile, a.chunk, a.breakdown)), flush=True)
 
 
 if __name__ == "__main__":

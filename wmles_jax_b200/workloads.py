@@ -232,7 +232,8 @@ def naca_cgrid_nodes(scale=1, far=NACA_FAR, span=NACA_SPAN, wall_spacing=2e-3):
     """Nodes (3, ni+1, nj+1, nk+1) of a four-block C-grid around the NACA 0012 section.
 
     One algebraic C-mesh: its inner line runs along the lower wake cut (x = far -> 1), around
-    the section (lower surface, leading edge, upper surface; cosine spacing) and along the
+    the section (lower surface, leading edge, upper surface; clustered at the leading edge)
+    and along the
     upper wake cut (1 -> far); its outer line is y = -far, a half circle of radius `far`
     about the trailing edge, and y = +far; nodes lie on straight lines between the two with
     geometric wall-normal spacing (first interval ~ wall_spacing).  It is cut into blocks
@@ -242,7 +243,11 @@ def naca_cgrid_nodes(scale=1, far=NACA_FAR, span=NACA_SPAN, wall_spacing=2e-3):
     40 spanwise cells over `span`.  `scale` divides every cell count."""
     n_wake, n_af, n_aft, nj, nk = 128 // scale, 320 // scale, 64 // scale, 64 // scale, 40 // scale
     s = np.linspace(0.0, 1.0, n_af + 1)
-    xa = 0.5 * (1.0 + np.cos(2.0 * np.pi * s))                      # 1 -> 0 -> 1
+    # per side x = 1 - sin(pi t / 2), t = distance from the trailing edge in index space:
+    # clustered at the leading edge, ~ chord / n_af at the trailing edge (a trailing-edge
+    # clustering would carry its fine x spacing out to the far field along the C-grid's
+    # trailing-edge lines, with cells of extreme aspect ratio there)
+    xa = 1.0 - np.sin(0.5 * np.pi * (1.0 - np.abs(1.0 - 2.0 * s)))  # 1 -> 0 -> 1
     ya = np.where(s <= 0.5, -1.0, 1.0) * naca0012_half_thickness(xa)
     xw = 1.0 + geometric_spacing(n_wake, 1.0 - xa[1], far - 1.0)     # 1 -> far
     phi = -0.5 * np.pi - np.pi * s
