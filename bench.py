@@ -36,9 +36,10 @@ sys.path.insert(0, ROOT)
 METRIC = "Mcell-steps/s"
 CONFIG_NAME = "channel 256x128x128, KEP4 + WALE + wall model + constant mass flux, SSP-RK3"
 N_CFG2 = (256, 128, 128)
-# DRAM bytes per stage-kernel launch per interior cell from one ncu capture of the same
-# kernel (profiles/stage_kernel_channel.md); None until captured
-TRAFFIC_PER_CELL = {"fp64": None, "mixed": None}
+# DRAM bytes (read + write) per stage-kernel launch per interior cell, mean of the three RK
+# stages, from one ncu capture of the same kernel on a 128^3 case of this workload
+# (profiles/stage_kernel_channel.md); scaled by the cell count for the roofline's `traffic`
+TRAFFIC_PER_CELL = {"fp64": 321.0, "mixed": 229.0}
 
 
 def peaks():
@@ -106,6 +107,30 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# ----------------------------------------------------------------------------- ranks
+def rank_barrier(dist):
+    """Barrier over the job's ranks (no-op for one process)."""
+    if dist is not None:
+        dist.barrier()
+
+
+def reduce_max(x, dist, device=None):
+    """Max of a per-rank float over all ranks (identity for one process): the job's time is
+    the slowest rank's."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_value(cells_per_rank, world, ms_per_step_max):
+    """Aggregate Mcell-steps/s of N replicas (weak scaling): every rank advances its own copy
+    of the workload, the job's step time is the slowest rank's."""
+    return cells_per_rank * world / (ms_per_step_max * 1e-3) / 1e6
+
+
 # ----------------------------------------------------------------------------- our arm
 def run_ours(args, rank, world, local_rank):
     import torch
@@ -121,15 +146,10 @@ def run_ours(args, rank, world, local_rank):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
+        rank_barrier(dist)
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, dist, dev)
 
     mesh, gas, kw, prim = channel_case(2, n=N_CFG2)
     cells = int(np.prod(mesh.blocks[0].n))
@@ -215,7 +235,7 @@ def run_ours(args, rank, world, local_rank):
     achieved = alg_launch / (f["stage_ms"] * 1e-3) / 1e9
     tr = TRAFFIC_PER_CELL["fp64"]
     line = {
-        "metric": METRIC, "value": cells * world / (f["ms"] * 1e-3) / 1e6, "unit": METRIC, "n_gpus": world,
+        "metric": METRIC, "value": whole_job_value(cells, world, f["ms"]), "unit": METRIC, "n_gpus": world,
         "steps": K, "warmup": Wm, "ms_per_step": f["ms"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded log-law IC + 10% noise)",
         "config": config_dict({"parallelism": f"replicas x{world}" if world > 1 else "1 GPU", "form": "fp64"}),
@@ -226,6 +246,8 @@ def run_ours(args, rank, world, local_rank):
         "roofline": {"bound": "hbm", "kernel": "stage_kernel<double,KEP>", "achieved": achieved, "peak": hbm,
                      "unit": "GB/s", "frac": achieved / hbm, "peak_source": f"{peak_kind} hbm_gbs",
                      "traffic": None if tr is None else tr * cells,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch on a 128^3 "
+                                       "case of the workload, per interior cell x cells",
                      "alg_bytes_per_launch": alg_launch, "mean_launch_ms": f["stage_ms"],
                      "whole_step_frac": (STEP_BYTES["fp64"] + CMF_BYTES) * cells / (f["ms"] * 1e-3) / 1e9 / hbm},
         "mixed": {"value": cells * world / (out["mixed"]["ms"] * 1e-3) / 1e6, "ms_per_step": out["mixed"]["ms"],

@@ -79,3 +79,13 @@ def test_serving_requests_seeded_mix():
         assert r.meta["grid"] in SERVING_GRIDS and r.dims == (r.meta["grid"],) and r.steps == 2000
     assert len({r.meta["grid"] for r in a}) == len(SERVING_GRIDS)
     assert serving_requests(seed=1)[0].arrival != a[0].arrival
+
+
+def test_backend_names_the_drivers_use():
+    from wmles_jax_b200 import backend
+    assert backend.HAS_JAX is False and hasattr(backend, "xp") and callable(backend.device_info)
+    import torch
+    if not torch.cuda.is_available():
+        assert backend.DEVICE is None
+        with pytest.raises(RuntimeError):
+            backend.asarray([1.0, 2.0])

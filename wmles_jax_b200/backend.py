@@ -36,3 +36,21 @@ def device_info():
     except Exception:  # pragma: no cover - torch import failure is reported by the solver
         pass
     return "cuda:unavailable"
+
+
+def asarray(value, dtype=None):
+    """``value`` as a tensor on the selected CUDA device (cf. wmles/backend.py:51-54, which
+    places arrays on the JAX device); NumPy dtype semantics for ``dtype``."""
+    import torch
+    return torch.from_numpy(xp.ascontiguousarray(xp.asarray(value, dtype=dtype))).to(require_gpu())
+
+
+def __getattr__(name):
+    # DEVICE (wmles/backend.py:32): the torch device of the cuda path, None without a GPU;
+    # resolved on access so that importing the package needs no GPU
+    if name == "DEVICE":
+        try:
+            return require_gpu()
+        except RuntimeError:
+            return None
+    raise AttributeError(name)
