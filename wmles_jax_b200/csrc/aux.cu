@@ -1,5 +1,6 @@
 // Surface and reduction kernels of the step: wall-model flux override, CFL time step with
 // the constant-mass-flux update, sponge spanwise means and synthetic-turbulence inflow.
+#include <algorithm>
 #include <cfloat>
 #include "physics.cuh"
 #include "aux.cuh"
@@ -100,6 +101,10 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
     return r;
 }
 
+template <typename M> __device__ __forceinline__ const M* metrics_of(const BlockDev& B);
+template <> __device__ __forceinline__ const double* metrics_of<double>(const BlockDev& B) { return B.met; }
+template <> __device__ __forceinline__ const float* metrics_of<float>(const BlockDev& B) { return B.met32; }
+
 // min that propagates NaN like NumPy's np.min (a NaN time step must not be masked)
 __device__ __forceinline__ double nanmin(double a, double b) { return (a != a || a < b) ? a : b; }
 
@@ -118,97 +123,118 @@ __device__ __forceinline__ double block_min(double v, double* red) {
 
 // CFL time step (Solver._dt, wmles/solver.py:135-151), optionally after applying the
 // constant-mass-flux shift (ConstantMassFlux.__call__, wmles/solver.py:22-36) in place.
-// One interior cell per thread over a flat grid of every block's CTAs; per-CTA minima,
-// reduced per case by the last CTA to finish.
+// The view's interior cells are cut into chunks of DT_NT cells, one cell per thread, chunks
+// numbered block by block; one wave of resident CTAs walks the chunks (grid stride) and
+// writes each chunk's minimum, and the last CTA to finish reduces the minima per case.
+// M: the metric copy read (double; float for the mixed form); the arithmetic and the
+// reduction are FP64 either way.
+template <typename M>
 __global__ void __launch_bounds__(DT_NT) dt_kernel(const __grid_constant__ DtArgs D) {
-    __shared__ double red[DT_NT / 32];
+    __shared__ double red[2][DT_NT / 32];
     __shared__ bool last;
-    int b = 0;
-    {
-        int hi = D.nblocks - 1;
-        while (b < hi) {             // last block whose first CTA is <= blockIdx.x
-            const int mid = (b + hi + 1) >> 1;
-            if (D.cta_start[mid] <= (int)blockIdx.x) b = mid; else hi = mid - 1;
-        }
-    }
-    const BlockDev& B = D.blocks[b];
-    const CaseDev& C = D.cases[B.case_id];
-    const bool cmf = D.cmf_delta != nullptr && C.cmf_dir >= 0;
-    const int ng = B.ng, nj = B.n[1], nk = B.n[2];
-    const int Nk = B.N[2];
-    const long long N = B.ncell, plane = B.plane;
-    const long long ncells = (long long)B.n[0] * nj * nk;
-    double dtmin = DBL_MAX;
-    const long long c = (long long)((int)blockIdx.x - D.cta_start[b]) * DT_NT + threadIdx.x;
-    if (c < ncells) {
-        double* q = D.q[b];
-        const double* met = B.met;
-        const int i = int(c / ((long long)nj * nk)) + ng;
-        const int r = int(c % ((long long)nj * nk));
-        const int j = r / nk + ng, k = r % nk + ng;
-        const long long idx = i * plane + (long long)j * Nk + k;
-        double qv[5];
-#pragma unroll
-        for (int v = 0; v < 5; ++v) qv[v] = q[v * N + idx];
-        // every metric this cell needs, read-only and issued before any store to q
-        const long long off[3] = {plane, Nk, 1};
-        double Sl[9], Sh[9];
-#pragma unroll
-        for (int d = 0; d < 3; ++d)
-#pragma unroll
-            for (int x = 0; x < 3; ++x) {
-                Sl[3 * d + x] = __ldg(met + (3 * d + x) * N + idx);
-                Sh[3 * d + x] = __ldg(met + (3 * d + x) * N + idx + off[d]);
+    int parity = 0;
+#pragma unroll 1
+    for (int chunk = blockIdx.x; chunk < D.ncta; chunk += gridDim.x) {
+        int b = 0;
+        {
+            int hi = D.nblocks - 1;
+            while (b < hi) {             // last block whose first chunk is <= chunk
+                const int mid = (b + hi + 1) >> 1;
+                if (D.cta_start[mid] <= chunk) b = mid; else hi = mid - 1;
             }
-        const double vol = __ldg(met + WM_MET_VOL * N + idx);
-        if (cmf) {
-            const double delta = D.cmf_delta[B.case_id];
-            const int m = 1 + C.cmf_dir;
-            const double dE = (2.0 * qv[m] * delta + delta * delta) / (2.0 * qv[0]);
-            qv[m] = qv[m] + delta;
-            qv[4] = qv[4] + dE;
-            q[m * N + idx] = qv[m];
-            q[4 * N + idx] = qv[4];
+        }
+        const BlockDev& B = D.blocks[b];
+        const CaseDev& C = D.cases[B.case_id];
+        const bool cmf = D.cmf_delta != nullptr && C.cmf_dir >= 0;
+        const int ng = B.ng, nj = B.n[1], nk = B.n[2];
+        const int Nk = B.N[2];
+        const long long N = B.ncell, plane = B.plane;
+        const long long ncells = (long long)B.n[0] * nj * nk;
+        double dtmin = DBL_MAX;
+        const long long c = (long long)(chunk - D.cta_start[b]) * DT_NT + threadIdx.x;
+        if (c < ncells) {
+            double* q = D.q[b];
+            const M* met = metrics_of<M>(B);
+            const int i = int(c / ((long long)nj * nk)) + ng;
+            const int r = int(c % ((long long)nj * nk));
+            const int j = r / nk + ng, k = r % nk + ng;
+            const long long idx = i * plane + (long long)j * Nk + k;
+            double qv[5];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) qv[v] = q[v * N + idx];
+            // every metric this cell needs, read-only and issued before any store to q
+            const long long off[3] = {plane, Nk, 1};
+            double Sl[9], Sh[9];
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+#pragma unroll
+                for (int x = 0; x < 3; ++x) {
+                    Sl[3 * d + x] = __ldg(met + (3 * d + x) * N + idx);
+                    Sh[3 * d + x] = __ldg(met + (3 * d + x) * N + idx + off[d]);
+                }
+            const double vol = __ldg(met + WM_MET_VOL * N + idx);
+            if (cmf) {
+                const double delta = D.cmf_delta[B.case_id];
+                const int m = 1 + C.cmf_dir;
+                const double dE = (2.0 * qv[m] * delta + delta * delta) / (2.0 * qv[0]);
+                qv[m] = qv[m] + delta;
+                qv[4] = qv[4] + dE;
+                q[m * N + idx] = qv[m];
+                q[4 * N + idx] = qv[4];
+            }
+            if (D.want_dt) {
+                const double rho = qv[0];
+                const double ir = 1.0 / rho, ivol = 1.0 / vol;
+                const double u = qv[1] * ir, v = qv[2] * ir, w = qv[3] * ir;
+                const double p = C.gm1 * (qv[4] - 0.5 * rho * ((u * u + v * v) + w * w));
+                const double T = p * ir * C.inv_Rg;
+                const double cs = sqrt(C.gamma * C.Rg * T);
+                const double nu = C.nu_fac * sutherland_d(T, C) * ir;
+                double lam = 0.0, lamv = 0.0;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const double sx = 0.5 * (Sl[3 * d] + Sh[3 * d]);
+                    const double sy = 0.5 * (Sl[3 * d + 1] + Sh[3 * d + 1]);
+                    const double sz = 0.5 * (Sl[3 * d + 2] + Sh[3 * d + 2]);
+                    const double Sm = sqrt((sx * sx + sy * sy) + sz * sz);
+                    lam = lam + fabs((u * sx + v * sy) + w * sz) + cs * Sm;
+                    lamv = lamv + nu * (Sm * Sm) * ivol;
+                }
+                dtmin = C.cfl * vol / (lam + 4.0 * lamv);
+            }
         }
         if (D.want_dt) {
-            const double rho = qv[0];
-            const double ir = 1.0 / rho, ivol = 1.0 / vol;
-            const double u = qv[1] * ir, v = qv[2] * ir, w = qv[3] * ir;
-            const double p = C.gm1 * (qv[4] - 0.5 * rho * ((u * u + v * v) + w * w));
-            const double T = p * ir * C.inv_Rg;
-            const double cs = sqrt(C.gamma * C.Rg * T);
-            const double nu = C.nu_fac * sutherland_d(T, C) * ir;
-            double lam = 0.0, lamv = 0.0;
+            // chunk minimum: warp shuffles, then one barrier; the two shared buffers alternate
+            // so the next chunk's writes never meet this chunk's read by thread 0
+            double m = dtmin;
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                const double sx = 0.5 * (Sl[3 * d] + Sh[3 * d]);
-                const double sy = 0.5 * (Sl[3 * d + 1] + Sh[3 * d + 1]);
-                const double sz = 0.5 * (Sl[3 * d + 2] + Sh[3 * d + 2]);
-                const double Sm = sqrt((sx * sx + sy * sy) + sz * sz);
-                lam = lam + fabs((u * sx + v * sy) + w * sz) + cs * Sm;
-                lamv = lamv + nu * (Sm * Sm) * ivol;
+            for (int o = 16; o > 0; o >>= 1) m = nanmin(m, __shfl_down_sync(0xffffffffu, m, o));
+            if ((threadIdx.x & 31) == 0) red[parity][threadIdx.x >> 5] = m;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double mm = DBL_MAX;
+                for (int w = 0; w < DT_NT / 32; ++w) mm = nanmin(mm, red[parity][w]);
+                D.dt_part[chunk] = mm;
             }
-            dtmin = C.cfl * vol / (lam + 4.0 * lamv);
+            parity ^= 1;
         }
     }
     if (!D.want_dt) return;
-    const double m = block_min<DT_NT>(dtmin, red);
     if (threadIdx.x == 0) {
-        D.dt_part[blockIdx.x] = m;
         __threadfence();
         const unsigned prev = atomicAdd(D.counter, 1u);
-        last = (prev == unsigned(D.ncta - 1));
+        last = (prev == gridDim.x - 1);
     }
     __syncthreads();
     if (last) {
-        // per case: the minimum over the CTAs of that case's blocks
+        // per case: the minimum over the chunks of that case's blocks
         __threadfence();
         for (int c = 0; c < D.ncases; ++c) {
             const int p0 = D.cta_start[D.case_block_start[c]];
             const int p1 = D.cta_start[D.case_block_start[c + 1]];
             double mm = DBL_MAX;
             for (int i = p0 + threadIdx.x; i < p1; i += DT_NT) mm = nanmin(mm, ((volatile double*)D.dt_part)[i]);
-            mm = block_min<DT_NT>(mm, red);
+            mm = block_min<DT_NT>(mm, red[0]);
             if (threadIdx.x == 0 && D.dt_out[c] != nullptr) D.dt_out[c][0] = mm;
             __syncthreads();
         }
@@ -216,8 +242,25 @@ __global__ void __launch_bounds__(DT_NT) dt_kernel(const __grid_constant__ DtArg
     }
 }
 
+// resident CTAs of one wave of dt_kernel<M> (computed once per process and metric type)
+template <typename M>
+static int dt_wave() {
+    static int ctas = 0;
+    if (ctas == 0) {
+        int dev = 0, sms = 148, per_sm = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dt_kernel<M>, DT_NT, 0);
+        ctas = sms * (per_sm > 0 ? per_sm : 1);
+    }
+    return ctas;
+}
+
 cudaError_t launch_dt(const DtArgs& D, cudaStream_t s) {
-    dt_kernel<<<D.ncta, DT_NT, 0, s>>>(D);
+    if (D.met32)
+        dt_kernel<float><<<std::min(D.ncta, dt_wave<float>()), DT_NT, 0, s>>>(D);
+    else
+        dt_kernel<double><<<std::min(D.ncta, dt_wave<double>()), DT_NT, 0, s>>>(D);
     return cudaGetLastError();
 }
 

@@ -28,13 +28,14 @@ struct DtArgs {
     const BlockDev* blocks;
     const CaseDev* cases;
     int nblocks;
-    int ncta;                              // one CTA per DT_NT interior cells of each block
-    int cta_start[WM_MAX_BLOCKS + 1];      // CTAs of block b: [cta_start[b], cta_start[b+1])
+    int ncta;                              // chunks of DT_NT interior cells, numbered block by block
+    int cta_start[WM_MAX_BLOCKS + 1];      // chunks of block b: [cta_start[b], cta_start[b+1])
     int ncases;
     int case_block_start[MAX_CASES + 1];   // blocks of case c: [start[c], start[c+1])
     double* q[WM_MAX_BLOCKS];      // state (modified in place when the constraint is applied)
     const double* cmf_delta;       // per case: constant-mass-flux shift from stage 3 (null: none)
     int want_dt;                   // 0: constraint only
+    int met32;                     // read the float metric copy (mixed form)
     double* dt_part;               // per-CTA minima
     unsigned int* counter;         // last-CTA-done counter (reset by the last CTA)
     double* dt_out[MAX_CASES];     // per case: time step

@@ -444,6 +444,7 @@ int run_dt(View* v, Prof* pf, double* const* q, bool apply_cmf, bool want_dt, do
     for (int b = 0; b < v->nblocks; ++b) D.q[b] = q[b];
     D.cmf_delta = apply_cmf ? v->cmf_delta : nullptr;
     D.want_dt = want_dt ? 1 : 0;
+    D.met32 = v->opts.precision == WM_PREC_MIXED ? 1 : 0;
     D.dt_part = v->dt_part; D.counter = v->counters;
     for (int ci = 0; ci < v->ncases; ++ci) D.dt_out[ci] = dt_out ? dt_out[ci] : nullptr;
     LaunchScope ls(pf, WM_KIND_DT, s);

@@ -232,7 +232,11 @@ __device__ __forceinline__ double spalding_utau(double kappa, double ekb, int n_
         const double ex = exp(ku);
         const double F = up + ekb * (ex - 1.0 - ku - 0.5 * ku * ku - ku * ku * ku / 6.0) - Reh / up;
         const double dF = 1.0 + ekb * kappa * (ex - 1.0 - ku - 0.5 * ku * ku) + Reh / (up * up);
-        up = fmin(fmax(up - F / dF, 0.5 * up), 100.0);
+        const double next = fmin(fmax(up - F / dF, 0.5 * up), 100.0);
+        // the update is a fixed function of up: once an iterate repeats exactly, every later
+        // one does too, so stopping here returns what all n_iter iterations would
+        if (next == up) break;
+        up = next;
     }
     return U / up;
 }
