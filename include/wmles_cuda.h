@@ -213,7 +213,10 @@ int wm_batch_info(wm_batch* b, int* nblocks, int* ntiles, long long* launches_pe
  * every launch on the launching stream; wm_profile_read waits for the recorded events and
  * returns the summed device time (ms) and the launch count of one kind (-1 = all kinds;
  * launch counts are kept even with timing disabled).  No reference counterpart: this is the
- * measurement hook of the benchmark. */
+ * measurement hook of the benchmark.  Kinds: STAGE the fused RHS + RK stage kernel; GHOST
+ * the surface launch before each stage (ghost cells, wall-model flux overrides, sponge
+ * means) and the ghost fill of wm_apply_bcs; WALL the wall model of wm_wall_stats; DT the
+ * CFL / constraint pass; SOURCE the synthetic-inflow fill. */
 enum { WM_KIND_STAGE = 0, WM_KIND_GHOST = 1, WM_KIND_WALL = 2, WM_KIND_DT = 3, WM_KIND_SOURCE = 4,
        WM_NKINDS = 5 };
 int wm_profile_enable(wm_case* c, int enable);

@@ -7,81 +7,6 @@
 
 namespace wm {
 
-__device__ __forceinline__ long long cell_index(const BlockDev& B, int axis, int c, int a, int b) {
-    // cell at position c along `axis`, (a, b) on the other two axes in increasing order
-    const int Nj = B.N[1], Nk = B.N[2];
-    if (axis == 0) return ((long long)c * Nj + a) * Nk + b;
-    if (axis == 1) return ((long long)a * Nj + c) * Nk + b;
-    return ((long long)a * Nj + b) * Nk + c;
-}
-
-__device__ __forceinline__ double sutherland_d(double T, const CaseDev& C) {
-    const double x = T * C.inv_Tref;
-    return C.mu_ref * (x * sqrt(x)) * C.TrefS / (T + C.S_suth);
-}
-
-// ------------------------------------------------------------------ wall model
-// WallModel.wall_flux (wmles/bc.py:145-166) with EquilibriumWallModel (wmles/wall_model.py:42-61)
-__global__ void wall_kernel(const __grid_constant__ WallArgs A) {
-    const WallDev& W = A.walls[blockIdx.y];
-    const long long nf = (long long)W.nt1 * W.nt2;
-    const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= nf) return;
-    const BlockDev& B = A.blocks[W.block];
-    const CaseDev& C = A.cases[B.case_id];
-    const int ng = B.ng, n = B.n[W.axis];
-    const int a = int(f / W.nt2) + ng, b = int(f % W.nt2) + ng;
-    const int mi = W.side == 0 ? ng + W.n_match - 1 : ng + n - W.n_match;
-    const int ci = W.side == 0 ? ng : ng + n - 1;
-    const double* q = A.q[W.block];
-    const long long N = B.ncell;
-    const long long im = cell_index(B, W.axis, mi, a, b), ic = cell_index(B, W.axis, ci, a, b);
-    const double rho = q[im];
-    const double u[3] = {q[N + im] / rho, q[2 * N + im] / rho, q[3 * N + im] / rho};
-    const double ke = (u[0] * u[0] + u[1] * u[1]) + u[2] * u[2];
-    const double p_h = C.gm1 * (q[4 * N + im] - 0.5 * rho * ke);
-    const double T_h = p_h / (rho * C.Rg);
-    const double rb = q[ic];
-    const double ub[3] = {q[N + ic] / rb, q[2 * N + ic] / rb, q[3 * N + ic] / rb};
-    const double p_b = C.gm1 * (q[4 * N + ic] - 0.5 * rb * ((ub[0] * ub[0] + ub[1] * ub[1]) + ub[2] * ub[2]));
-    const double Sm = W.geom[f], nrm[3] = {W.geom[nf + f], W.geom[2 * nf + f], W.geom[3 * nf + f]};
-    const double h = W.geom[4 * nf + f];
-    const double un = (u[0] * nrm[0] + u[1] * nrm[1]) + u[2] * nrm[2];
-    const double up[3] = {u[0] - un * nrm[0], u[1] - un * nrm[1], u[2] - un * nrm[2]};
-    const double U = sqrt((up[0] * up[0] + up[1] * up[1]) + up[2] * up[2] + 1e-20);
-    // equilibrium model
-    const double Um = fmax(U, 1e-8);
-    const double T_w = W.isothermal ? W.T_wall : T_h + C.Pr13 * (Um * Um) / (2.0 * C.cp);
-    const double rho_w = p_h / (C.Rg * T_w);
-    const double mu_w = sutherland_d(T_w, C);
-    const double ut = spalding_utau(W.kappa, W.ekb, W.n_iter, h, Um, rho_w, mu_w);
-    const double tau = rho_w * (ut * ut);
-    double qw = 0.0;
-    if (W.isothermal) {
-        // Kader (1981) temperature law
-        const double Pr = C.Pr;
-        const double yp = fmax(h * ut * rho_w / mu_w, 1e-6);
-        const double x = Pr * yp, x2 = x * x;
-        const double Gam = fmax(0.01 * (x2 * x2) / (1.0 + 5.0 * C.Pr3 * yp), 1e-20);
-        const double Tp = Pr * yp * exp(-Gam) + (2.12 * log(1.0 + yp) + C.kader_beta) * exp(-1.0 / Gam);
-        qw = rho_w * C.cp * ut * (T_w - T_h) / Tp;
-    }
-    const double sgn = W.side == 1 ? 1.0 : -1.0;
-    W.F[f] = 0.0;
-#pragma unroll
-    for (int v = 0; v < 3; ++v) W.F[(1 + v) * nf + f] = sgn * ((p_b * nrm[v] + tau * (up[v] / U)) * Sm);
-    W.F[4 * nf + f] = sgn * (-qw * Sm);
-    W.tq[f] = tau;
-    W.tq[nf + f] = qw;
-}
-
-cudaError_t launch_wall(const WallArgs& W, cudaStream_t s) {
-    if (W.nwalls == 0) return cudaSuccess;
-    dim3 grid((W.max_faces + 127) / 128, W.nwalls);
-    wall_kernel<<<grid, 128, 0, s>>>(W);
-    return cudaGetLastError();
-}
-
 // ------------------------------------------------------------------ reductions
 template <int NT>
 __device__ __forceinline__ double block_sum(double v, double* red) {
@@ -261,48 +186,6 @@ cudaError_t launch_dt(const DtArgs& D, cudaStream_t s) {
         dt_kernel<float><<<std::min(D.ncta, dt_wave<float>()), DT_NT, 0, s>>>(D);
     else
         dt_kernel<double><<<std::min(D.ncta, dt_wave<double>()), DT_NT, 0, s>>>(D);
-    return cudaGetLastError();
-}
-
-// ------------------------------------------------------------------ sponge
-// volume-weighted spanwise mean of q over interior k, per interior (i, j) row
-// (SmoothRampSponge.__call__, wmles/smooth_ramp.py:212-216)
-__global__ void sponge_mean_kernel(const __grid_constant__ SpongeArgs S) {
-    const int b = blockIdx.y;
-    if (S.mean[b] == nullptr) return;    // block of a case without a sponge
-    const BlockDev& B = S.blocks[b];
-    const int ng = B.ng, ni = B.n[0], nj = B.n[1], nk = B.n[2];
-    const int row = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
-    if (row >= ni * nj) return;
-    const int lane = threadIdx.x & 31;
-    const int i = row / nj + ng, j = row % nj + ng;
-    const long long N = B.ncell;
-    const long long base = i * B.plane + (long long)j * B.N[2];
-    const double* q = S.q[b];
-    double acc[5] = {0, 0, 0, 0, 0}, vs = 0.0;
-    for (int k = ng + lane; k < ng + nk; k += 32) {
-        const double vol = B.met[WM_MET_VOL * N + base + k];
-        vs += vol;
-#pragma unroll
-        for (int v = 0; v < 5; ++v) acc[v] += q[v * N + base + k] * vol;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        vs += __shfl_down_sync(0xffffffffu, vs, o);
-#pragma unroll
-        for (int v = 0; v < 5; ++v) acc[v] += __shfl_down_sync(0xffffffffu, acc[v], o);
-    }
-    if (lane == 0) {
-        const long long mn = (long long)B.N[0] * B.N[1];
-        const long long mi = (long long)i * B.N[1] + j;
-#pragma unroll
-        for (int v = 0; v < 5; ++v) S.mean[b][v * mn + mi] = acc[v] / vs;
-    }
-}
-
-cudaError_t launch_sponge_mean(const SpongeArgs& S, int max_rows, cudaStream_t s) {
-    dim3 grid((max_rows + 3) / 4, S.nblocks);
-    sponge_mean_kernel<<<grid, 128, 0, s>>>(S);
     return cudaGetLastError();
 }
 

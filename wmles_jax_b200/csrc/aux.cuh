@@ -59,7 +59,31 @@ struct InflowArgs {
     double* out;             // 5 x (ng * Nj * Nk)
 };
 
+// before each stage kernel: ghost gather (single phase), wall model and sponge means in one
+// launch; the CTA counts are filled in by the launcher (an empty part has none)
+struct SurfaceArgs {
+    GhostArgs G;
+    WallArgs W;
+    SpongeArgs S;          // nblocks = 0: no sponge
+    int g_ctas, w_per, w_ctas, s_per;
+};
+
+__device__ __forceinline__ long long cell_index(const BlockDev& B, int axis, int c, int a, int b) {
+    // cell at position c along `axis`, (a, b) on the other two axes in increasing order
+    const int Nj = B.N[1], Nk = B.N[2];
+    if (axis == 0) return ((long long)c * Nj + a) * Nk + b;
+    if (axis == 1) return ((long long)a * Nj + c) * Nk + b;
+    return ((long long)a * Nj + b) * Nk + c;
+}
+
+// Sutherland viscosity in FP64 (wmles/gas.py:39-41)
+__device__ __forceinline__ double sutherland_d(double T, const CaseDev& C) {
+    const double x = T * C.inv_Tref;
+    return C.mu_ref * (x * sqrt(x)) * C.TrefS / (T + C.S_suth);
+}
+
 cudaError_t launch_ghost(const GhostArgs& G, cudaStream_t s);
+cudaError_t launch_surface(SurfaceArgs& A, int max_sponge_rows, cudaStream_t s);
 cudaError_t launch_wall(const WallArgs& W, cudaStream_t s);
 cudaError_t launch_dt(const DtArgs& D, cudaStream_t s);
 cudaError_t launch_sponge_mean(const SpongeArgs& S, int max_rows, cudaStream_t s);

@@ -383,34 +383,28 @@ int run_stage(View* v, Prof* pf, int stage, double* const* q_in, const double* c
               const double* const* dt, const double* times, double time_dt, cudaStream_t s) {
     int r;
     if ((r = fill_inflow(v, pf, times, time_dt, dt, s))) return r;
-    {
-        GhostArgs G{};
-        G.segs = v->d_seg_rhs; G.nseg = v->ncases; G.total = v->total_rhs; G.stash = nullptr;
-        for (int b = 0; b < v->nblocks; ++b) { G.q[b] = q_in[b]; G.ncell[b] = v->hb[b].ncell; }
-        LaunchScope ls(pf, WM_KIND_GHOST, s, G.total ? 1 : 0);
-        CK(launch_ghost(G, s));
-    }
-    if (!v->hw.empty()) {
-        WallArgs W{};
-        W.blocks = v->d_blocks; W.cases = v->d_cases; W.walls = v->d_walls;
-        W.nwalls = (int)v->hw.size(); W.max_faces = v->max_wall_faces;
-        for (int b = 0; b < v->nblocks; ++b) W.q[b] = q_in[b];
-        LaunchScope ls(pf, WM_KIND_WALL, s);
-        CK(launch_wall(W, s));
-    }
+    // ghost cells the RHS reads, wall-model flux overrides and sponge means: one launch
+    SurfaceArgs U{};
+    U.G.segs = v->d_seg_rhs; U.G.nseg = v->ncases; U.G.total = v->total_rhs; U.G.stash = nullptr;
+    for (int b = 0; b < v->nblocks; ++b) { U.G.q[b] = q_in[b]; U.G.ncell[b] = v->hb[b].ncell; }
+    U.W.blocks = v->d_blocks; U.W.cases = v->d_cases; U.W.walls = v->d_walls;
+    U.W.nwalls = (int)v->hw.size(); U.W.max_faces = v->max_wall_faces;
+    for (int b = 0; b < v->nblocks; ++b) U.W.q[b] = q_in[b];
     std::vector<const double*> spm(v->nblocks, nullptr);
     if (v->any_sponge) {
-        SpongeArgs S{};
-        S.blocks = v->d_blocks; S.nblocks = v->nblocks;
+        U.S.blocks = v->d_blocks; U.S.nblocks = v->nblocks;
         for (int ci = 0; ci < v->ncases; ++ci)
             for (size_t b = 0; b < v->members[ci]->hb.size(); ++b) {
                 const int vb = v->case_block_start[ci] + (int)b;
-                S.q[vb] = q_in[vb];
-                S.mean[vb] = v->members[ci]->spmean[b];
-                spm[vb] = S.mean[vb];
+                U.S.q[vb] = q_in[vb];
+                U.S.mean[vb] = v->members[ci]->spmean[b];
+                spm[vb] = U.S.mean[vb];
             }
-        LaunchScope ls(pf, WM_KIND_SOURCE, s);
-        CK(launch_sponge_mean(S, v->sponge_rows, s));
+    }
+    {
+        const bool any = U.G.total > 0 || !v->hw.empty() || v->any_sponge;
+        LaunchScope ls(pf, WM_KIND_GHOST, s, any ? 1 : 0);
+        CK(launch_surface(U, v->sponge_rows, s));
     }
     StageArgs A{};
     A.blocks = v->d_blocks; A.cases = v->d_cases; A.walls = v->d_walls;
@@ -702,7 +696,7 @@ int wm_batch_info(wm_batch* b, int* nblocks, int* ntiles, long long* launches_pe
     const View& v = b->view;
     int inflow = 0;
     for (wm_case* c : v.members) inflow += c->has_inflow ? 1 : 0;
-    const long long per_stage = inflow + (v.total_rhs ? 1 : 0) + (v.hw.empty() ? 0 : 1) + (v.any_sponge ? 1 : 0) + 1;
+    const long long per_stage = inflow + ((v.total_rhs || !v.hw.empty() || v.any_sponge) ? 1 : 0) + 1;
     if (nblocks) *nblocks = v.nblocks;
     if (ntiles) *ntiles = (int)v.tiles.size();
     if (launches_per_step) *launches_per_step = 3 * per_stage + 1;

@@ -57,8 +57,9 @@ def run(config, precision, steps, n=None, scale=1, tile=None, chunk=None, breakd
            "steps": steps, "ms_per_step": el * 1e3, "mcell_steps_per_s": cells / el / 1e6, "time": t,
            "finite": all(bool(torch.isfinite(q).all()) for q in Q)}
     if breakdown:
-        names = {N.KIND_STAGE: "stage", N.KIND_GHOST: "ghost", N.KIND_WALL: "wall", N.KIND_DT: "dt",
-                 N.KIND_SOURCE: "source"}
+        # "surface": ghost cells + wall-model overrides + sponge means, one launch per stage
+        names = {N.KIND_STAGE: "stage", N.KIND_GHOST: "surface", N.KIND_WALL: "wall_stats", N.KIND_DT: "dt",
+                 N.KIND_SOURCE: "inflow"}
         out["device_ms_per_step"] = {names[k]: s.profile_read(k)[0] / steps for k in names}
         out["launches_per_step"] = s.profile_read(-1)[1] / steps
     return out
