@@ -219,21 +219,25 @@ __global__ void __launch_bounds__(IN_NT) inflow_kernel(const __grid_constant__ I
     const double time = I.time0 + I.time_dt * (I.dt ? *I.dt : 0.0);
     const double X = I.U_inf * time / I.L;
     double* f0 = fsm;
-    for (int c = 0; c < 3; ++c) {
-        double* f = fsm + c * Nk;
+    // raw mode sums of all three components at once: one (component, k) pair per thread
+    for (int it = threadIdx.x; it < 3 * Nk; it += IN_NT) {
+        const int c = it / Nk, k = it - c * Nk;
         const double* kx = I.modes + (c * 4 + 0) * I.n_modes;
         const double* ky = I.modes + (c * 4 + 1) * I.n_modes;
         const double* kz = I.modes + (c * 4 + 2) * I.n_modes;
         const double* ph = I.modes + (c * 4 + 3) * I.n_modes;
+        const long long idx = ((long long)gi * Nj + j) * Nk + k;
+        const double y = B.met[WM_MET_XCY * N + idx] / I.L, z = B.met[WM_MET_XCZ * N + idx] / I.L;
+        double acc = 0.0;
+        for (int q = 0; q < I.n_modes; ++q) acc += cos(((kx[q] * X + ky[q] * y) + kz[q] * z) + ph[q]);
+        fsm[c * Nk + k] = acc;
+    }
+    __syncthreads();
+    for (int c = 0; c < 3; ++c) {
+        double* f = fsm + c * Nk;
         double s_int = 0.0;
-        for (int k = threadIdx.x; k < Nk; k += IN_NT) {
-            const long long idx = ((long long)gi * Nj + j) * Nk + k;
-            const double y = B.met[WM_MET_XCY * N + idx] / I.L, z = B.met[WM_MET_XCZ * N + idx] / I.L;
-            double acc = 0.0;
-            for (int q = 0; q < I.n_modes; ++q) acc += cos(((kx[q] * X + ky[q] * y) + kz[q] * z) + ph[q]);
-            f[k] = acc;
-            if (k >= ng && k < ng + nk) s_int += acc;
-        }
+        for (int k = threadIdx.x; k < Nk; k += IN_NT)
+            if (k >= ng && k < ng + nk) s_int += f[k];
         const double mean = block_sum<IN_NT>(s_int, red) / nk;
         double cov_acc = 0.0;
         for (int k = threadIdx.x; k < Nk; k += IN_NT) {
