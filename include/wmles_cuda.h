@@ -21,6 +21,7 @@
  *   wm_advance       Solver.advance             wmles/solver.py:110-133,156-157
  *   wm_step          max_dt + advance, as the drivers call them (examples/channel_wmles.py:124-125)
  *   wm_wall_stats    Solver.wall_stats          wmles/solver.py:163-179
+ *   wm_plane_stats   PlaneStats.accumulate      wmles/channel5200.py:121-152
  */
 #ifndef WMLES_CUDA_H
 #define WMLES_CUDA_H
@@ -185,6 +186,14 @@ int wm_max_dt_noalloc(int nblocks, const int* dims, const double* const* q, cons
 
 /* (tau_w, q_w) of every wall-modelled face: out[w] is a device buffer of 2 x nt1 x nt2. */
 int wm_wall_stats(wm_case* c, const double* const* q, double* const* out, void* stream);
+
+/* Plane statistics of block `block` (PlaneStats.accumulate, wmles/channel5200.py:121-152):
+ * for every interior j-plane, the means over interior (i, k) of rho, u, v, w, uu, vv, ww, uv,
+ * uw, vw, T and p are ADDED to sum (device, 12 x nj doubles, quantity-major), so a driver
+ * samples the flow on the device; q is the block's state (ghost cells are not read).  The
+ * block must have the same y on every (i, k) of a plane (an unskewed channel block), as in
+ * the reference. */
+int wm_plane_stats(wm_case* c, int block, const double* q, double* sum, void* stream);
 
 /* Batched stepping of several resident cases (no reference counterpart: the reference
  * advances one case per Solver).  A wm_batch is a fixed set of cases that share the

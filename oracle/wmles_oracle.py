@@ -601,3 +601,16 @@ def sponge_source(src, blk, q, geom):
 def init_state(solver, prim_fn):
     """wmles/solver.py:54-56 (host arrays)."""
     return tuple(prim_to_cons(solver.gas, np.asarray(prim_fn(g.xc), float)) for g in solver.geoms)
+
+
+def plane_means(gas, blk, q):
+    """Per interior j-plane means over interior (i, k) of rho, u, v, w, uu, vv, ww, uv, uw,
+    vw, T, p for one sample of one block; PlaneStats.accumulate, wmles/channel5200.py:135-151."""
+    w, T = cons_to_prim(gas, q)
+    u, v, wc = (blk.interior(c) for c in w[1:4])
+    rho, Ta, p = blk.interior(w[0]), blk.interior(T), blk.interior(w[4])
+    ax = (0, 2)
+    return {"rho": rho.mean(axis=ax), "u": u.mean(axis=ax), "v": v.mean(axis=ax), "w": wc.mean(axis=ax),
+            "uu": (u * u).mean(axis=ax), "vv": (v * v).mean(axis=ax), "ww": (wc * wc).mean(axis=ax),
+            "uv": (u * v).mean(axis=ax), "uw": (u * wc).mean(axis=ax), "vw": (v * wc).mean(axis=ax),
+            "T": Ta.mean(axis=ax), "p": p.mean(axis=ax)}

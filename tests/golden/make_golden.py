@@ -117,6 +117,30 @@ def main():
     np.savez_compressed(os.path.join(HERE, "golden_cases.npz"), **out)
     print("wrote golden_cases.npz:", len(out), "arrays")
 
+    # ---------------------------------------------------------------- plane statistics
+    # the reference's PlaneStats (wmles/channel5200.py:121-199) over two samples of the
+    # small constant-mass-flux channel: the initial state and the state after one step
+    from wmles.channel5200 import PlaneStats
+    mesh, gas, kw, prim, t = C.golden_case(W, "channel_small_cmf")
+    solver = W.Solver(mesh, gas, **kw)
+    Q0 = solver.init_state(prim)
+    Q1 = solver.advance(Q0, float(solver.max_dt(Q0)))
+    ps = PlaneStats(mesh, solver)
+    ps.accumulate(Q0)
+    ps.accumulate(Q1)
+    y, avg = ps.result()
+    outp = {"y": np.asarray(y), "mean_tau_w": np.array(ps.mean_tau_w), "mu_ref": np.array(gas.mu_ref)}
+    for ib, (a, b) in enumerate(zip(Q0, Q1)):
+        outp[f"q0_{ib}"], outp[f"q1_{ib}"] = np.asarray(a), np.asarray(b)
+    for k, v in avg.items():
+        outp[f"avg/{k}"] = np.asarray(v)
+    u_tau, wu = ps.wall_units(ps.mean_tau_w, 1.0, gas.mu_ref, 1.0)
+    outp["wu/u_tau"] = np.array(u_tau)
+    for k, v in wu.items():
+        outp[f"wu/{k}"] = np.asarray(v)
+    np.savez_compressed(os.path.join(HERE, "golden_planestats.npz"), **outp)
+    print("wrote golden_planestats.npz:", len(outp), "arrays")
+
     # ---------------------------------------------------------------- config-1 channel, 100 steps
     if args.skip_cfg1:
         return

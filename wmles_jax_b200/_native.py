@@ -73,6 +73,7 @@ SIGNATURES = {
     "wm_max_dt_noalloc": (C.c_int, [C.c_int, c_int_p, PP, PP, C.POINTER(WmGas), C.c_double, c_double_p,
                                     C.c_void_p]),
     "wm_wall_stats": (C.c_int, [C.c_void_p, PP, PP, C.c_void_p]),
+    "wm_plane_stats": (C.c_int, [C.c_void_p, C.c_int, c_double_p, c_double_p, C.c_void_p]),
     "wm_batch_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     "wm_batch_destroy": (None, [C.c_void_p]),
     "wm_batch_step": (C.c_int, [C.c_void_p, PP, PP, PP, PP, c_double_p, C.c_void_p]),

@@ -20,6 +20,7 @@
 #include "wm_internal.cuh"
 #include "stage.cuh"
 #include "aux.cuh"
+#include "stats.cuh"
 
 using namespace wm;
 
@@ -154,6 +155,8 @@ struct wm_case {
     wm_inflow inflow{};
     long long inflow_n = 0;
     std::vector<double*> spmean;         // per block, null without sponge
+    double* ps_part = nullptr;           // plane-statistics scratch (PS_NQ x max Nj x PS_CHUNKS)
+    unsigned* ps_counter = nullptr;
     View* self = nullptr;                // the case as a view of one case
     Prof prof;
     ~wm_case();
@@ -595,6 +598,13 @@ int wm_case_create(const wm_case_desc* d, wm_case** out) {
 
     c->chunk_req = d->chunk > 0 ? d->chunk : 0;
 
+    // ---- plane-statistics scratch
+    int max_nj = 1;
+    for (const BlockDev& B : c->hb) max_nj = std::max(max_nj, B.n[1]);
+    if ((r = c->mem.alloc(&c->ps_part, (size_t)PS_NQ * max_nj * PS_CHUNKS))) return bail(r);
+    if ((r = c->mem.alloc(&c->ps_counter, 1))) return bail(r);
+    CK(cudaMemset(c->ps_counter, 0, sizeof(unsigned)));
+
     c->self = new View();
     wm_case* self_list[1] = {c};
     if ((r = build_view(c->self, self_list, 1))) return bail(r);
@@ -664,6 +674,22 @@ int wm_wall_stats(wm_case* c, const double* const* q, double* const* out, void* 
         const size_t nf = (size_t)v->hw[w].nt1 * v->hw[w].nt2;
         CK(cudaMemcpyAsync(out[w], v->hw[w].tq, sizeof(double) * 2 * nf, cudaMemcpyDeviceToDevice, s));
     }
+    return WM_OK;
+}
+
+int wm_plane_stats(wm_case* c, int block, const double* q, double* sum, void* stream) {
+    if (!c || !q || !sum) return fail(WM_E_INVALID, "null argument");
+    if (block < 0 || block >= c->self->nblocks) return fail(WM_E_INVALID, "block %d out of range", block);
+    PlaneStatsArgs A{};
+    A.block = c->self->d_blocks + block;
+    A.q = q;
+    A.gm1 = c->hc.gm1;
+    A.Rg = c->hc.Rg;
+    A.nchunks = PS_CHUNKS;
+    A.part = c->ps_part;
+    A.sum = sum;
+    A.counter = c->ps_counter;
+    CK(launch_plane_stats(A, c->hb[block].n[1], (cudaStream_t)stream));
     return WM_OK;
 }
 

@@ -291,6 +291,14 @@ class Solver:
     def wall_stats(self, Q):
         """{(block, face): (tau_w, q_w)} host arrays for every wall-modelled face
         (wmles/solver.py:163-179)."""
+        out = {}
+        for key, buf in self.wall_stats_device(Q).items():
+            h = buf.cpu().numpy()
+            out[key] = (h[0], h[1])
+        return out
+
+    def wall_stats_device(self, Q):
+        """{(block, face): tensor (2, nt1, nt2) of (tau_w, q_w)} on the device, no host copy."""
         self._check_state(Q)
         bufs = []
         for ib, a, s, bc in self.walls:
@@ -300,11 +308,8 @@ class Solver:
         if not bufs:
             return {}
         N.check(self._lib.wm_wall_stats(self._case, self._ptrs(Q), self._ptrs(bufs), self._stream()), "wm_wall_stats")
-        out = {}
-        for (ib, a, s, bc), buf in zip(self.walls, bufs):
-            h = buf.cpu().numpy()
-            out[(self.blocks[ib].name, "ijk"[a] + ("min", "max")[s])] = (h[0], h[1])
-        return out
+        return {(self.blocks[ib].name, "ijk"[a] + ("min", "max")[s]): buf
+                for (ib, a, s, bc), buf in zip(self.walls, bufs)}
 
     def wall_loads(self, Q, moment_center=(0.0, 0.0, 0.0)):
         """Integrated fluid-on-wall force and moment per wall-modelled face
