@@ -260,6 +260,7 @@ def run_ours(args, rank, world, local_rank):
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.cpu_cells)
     if world == 1 and args.extra:
+        line["diagnostics"] = diagnostics_leg(mesh, s64, Q64, cells)
         del s64, s32, Q64, Q32, Qn, dbuf
         line["mixed"]["error_vs_fp64"] = precision_leg()
         line["configs"] = configs_leg()
@@ -285,6 +286,41 @@ def configs_leg(steps=100):
                                "finite": r["fp64"]["finite"] and r["mixed"]["finite"],
                                "timing": "host clock around steps (the time advances by the returned dt each step)"}
     return out
+
+
+def diagnostics_leg(mesh, solver, Q, cells, samples=20):
+    """Device cost of sampling the flow: PlaneStats.accumulate (per-plane means over the whole
+    block, plus the wall shear of both walls) on the config-2 state, CUDA events around
+    `samples` calls; algorithmic bytes = the state's 40 B per interior cell."""
+    import torch
+    from wmles_jax_b200.stats import PlaneStats
+    hbm, _ = peaks()
+    ps = PlaneStats(mesh, solver)
+    for _ in range(3):
+        ps.accumulate(Q)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(samples):
+        ps.accumulate(Q)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / samples
+    from wmles_jax_b200.output import derived_fields
+    for _ in range(2):
+        derived_fields(solver, Q, as_numpy=False)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(5):
+        derived_fields(solver, Q, as_numpy=False)
+    e1.record()
+    torch.cuda.synchronize()
+    dms = e0.elapsed_time(e1) / 5
+    return {"plane_stats_ms_per_sample": ms, "plane_stats_hbm_frac": 40.0 * cells / (ms * 1e-3) / 1e9 / hbm,
+            "derived_fields_ms": dms,
+            "what": "wmles_jax_b200.stats.PlaneStats.accumulate (12 plane means + mean wall shear) and "
+                    "wmles_jax_b200.output.derived_fields (apply_bcs + 11 fields per cell, kept on the device) "
+                    "on the 256x128x128 state"}
 
 
 def precision_leg():

@@ -22,6 +22,7 @@
  *   wm_step          max_dt + advance, as the drivers call them (examples/channel_wmles.py:124-125)
  *   wm_wall_stats    Solver.wall_stats          wmles/solver.py:163-179
  *   wm_plane_stats   PlaneStats.accumulate      wmles/channel5200.py:121-152
+ *   wm_derived_fields derived_fields            wmles/io_vtk.py:269-293
  */
 #ifndef WMLES_CUDA_H
 #define WMLES_CUDA_H
@@ -33,6 +34,7 @@ extern "C" {
 #define WM_ABI_VERSION 1
 #define WM_MAX_BLOCKS 96      /* blocks per case (all cases of one batched launch) */
 #define WM_NMET 27            /* metric components per cell, see WM_MET_* */
+#define WM_NDERIVED 11        /* derived output fields per cell, see wm_derived_fields */
 
 /* status codes */
 #define WM_OK 0
@@ -194,6 +196,13 @@ int wm_wall_stats(wm_case* c, const double* const* q, double* const* out, void* 
  * block must have the same y on every (i, k) of a plane (an unskewed channel block), as in
  * the reference. */
 int wm_plane_stats(wm_case* c, int block, const double* q, double* sum, void* stream);
+
+/* Derived output fields of every block (derived_fields, wmles/io_vtk.py:269-293): out[b] is
+ * a device array of WM_NDERIVED x ni x nj x nk doubles (interior only) receiving rho, u, v,
+ * w, p, T, Mach number, SGS viscosity mu_t, molecular viscosity mu, vorticity magnitude and
+ * Q-criterion.  q must have its first ghost layer filled (call wm_apply_bcs first, as the
+ * reference does); it is not modified. */
+int wm_derived_fields(wm_case* c, const double* const* q, double* const* out, void* stream);
 
 /* Batched stepping of several resident cases (no reference counterpart: the reference
  * advances one case per Solver).  A wm_batch is a fixed set of cases that share the

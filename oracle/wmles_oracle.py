@@ -614,3 +614,26 @@ def plane_means(gas, blk, q):
             "uu": (u * u).mean(axis=ax), "vv": (v * v).mean(axis=ax), "ww": (wc * wc).mean(axis=ax),
             "uv": (u * v).mean(axis=ax), "uw": (u * wc).mean(axis=ax), "vw": (v * wc).mean(axis=ax),
             "T": Ta.mean(axis=ax), "p": p.mean(axis=ax)}
+
+
+def derived_fields(solver, Q):
+    """{block: {name: interior array}} of rho, velocity, pressure, temperature, Mach, mu_t,
+    mu, |omega| and Q-criterion; wmles/io_vtk.py:269-293 (ghost cells filled first)."""
+    gas = solver.gas
+    Q = solver.apply_bcs(Q)
+    out = {}
+    for ib, (blk, q, geom) in enumerate(zip(solver.blocks, Q, solver.geoms)):
+        w, T = cons_to_prim(gas, q)
+        mu = viscosity(gas, T)
+        g = green_gauss(w[1:4], geom)
+        mut = 0.0 * w[0] if solver.sgs.name == "none" else w[0] * sgs_nut(solver.sgs, g, geom.vol ** (1.0 / 3.0))
+        wxy, wxz, wyz = g[1, 0] - g[0, 1], g[2, 0] - g[0, 2], g[2, 1] - g[1, 2]
+        omega = np.sqrt(wxy ** 2 + wxz ** 2 + wyz ** 2)
+        S = 0.5 * (g + np.swapaxes(g, 0, 1))
+        Om = 0.5 * (g - np.swapaxes(g, 0, 1))
+        qcrit = 0.5 * (np.sum(Om ** 2, axis=(0, 1)) - np.sum(S ** 2, axis=(0, 1)))
+        mach = np.sqrt(np.sum(w[1:4] ** 2, axis=0)) / sound_speed(gas, T)
+        out[ib] = {"rho": blk.interior(w[0]), "velocity": blk.interior(w[1:4]), "pressure": blk.interior(w[4]),
+                   "temperature": blk.interior(T), "mach": blk.interior(mach), "mu_t": blk.interior(mut),
+                   "mu": blk.interior(mu), "vorticity_mag": blk.interior(omega), "q_criterion": blk.interior(qcrit)}
+    return out

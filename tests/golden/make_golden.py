@@ -141,6 +141,21 @@ def main():
     np.savez_compressed(os.path.join(HERE, "golden_planestats.npz"), **outp)
     print("wrote golden_planestats.npz:", len(outp), "arrays")
 
+    # ---------------------------------------------------------------- derived output fields
+    # the reference's derived_fields (wmles/io_vtk.py:269-293; pyvista is not needed for it)
+    # on two skewed split blocks with the wall model and WALE, and on the NACA C-grid (Vreman)
+    from wmles.io_vtk import derived_fields
+    outd = {}
+    for tag in ("split_wm_hybrid", "naca_small"):
+        mesh, gas, kw, prim, t = C.golden_case(W, tag)
+        solver = W.Solver(mesh, gas, **kw)
+        Q = tuple(out[f"{tag}/q{ib}"] for ib in range(len(mesh.blocks)))
+        for ib, fields in derived_fields(solver, Q).items():
+            for k, v in fields.items():
+                outd[f"{tag}/{ib}/{k}"] = np.asarray(v)
+    np.savez_compressed(os.path.join(HERE, "golden_derived.npz"), **outd)
+    print("wrote golden_derived.npz:", len(outd), "arrays")
+
     # ---------------------------------------------------------------- config-1 channel, 100 steps
     if args.skip_cfg1:
         return

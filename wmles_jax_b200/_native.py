@@ -74,6 +74,7 @@ SIGNATURES = {
                                     C.c_void_p]),
     "wm_wall_stats": (C.c_int, [C.c_void_p, PP, PP, C.c_void_p]),
     "wm_plane_stats": (C.c_int, [C.c_void_p, C.c_int, c_double_p, c_double_p, C.c_void_p]),
+    "wm_derived_fields": (C.c_int, [C.c_void_p, PP, PP, C.c_void_p]),
     "wm_batch_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     "wm_batch_destroy": (None, [C.c_void_p]),
     "wm_batch_step": (C.c_int, [C.c_void_p, PP, PP, PP, PP, c_double_p, C.c_void_p]),
@@ -82,6 +83,7 @@ SIGNATURES = {
     "wm_profile_read": (C.c_int, [C.c_void_p, C.c_int, c_double_p, C.POINTER(C.c_longlong)]),
 }
 KIND_STAGE, KIND_GHOST, KIND_WALL, KIND_DT, KIND_SOURCE = range(5)
+NDERIVED = 11
 
 _lib = None
 

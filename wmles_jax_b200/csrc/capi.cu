@@ -21,6 +21,7 @@
 #include "stage.cuh"
 #include "aux.cuh"
 #include "stats.cuh"
+#include "derived.cuh"
 
 using namespace wm;
 
@@ -690,6 +691,22 @@ int wm_plane_stats(wm_case* c, int block, const double* q, double* sum, void* st
     A.sum = sum;
     A.counter = c->ps_counter;
     CK(launch_plane_stats(A, c->hb[block].n[1], (cudaStream_t)stream));
+    return WM_OK;
+}
+
+int wm_derived_fields(wm_case* c, const double* const* q, double* const* out, void* stream) {
+    if (!c || !q || !out) return fail(WM_E_INVALID, "null argument");
+    View* v = c->self;
+    for (int b = 0; b < v->nblocks; ++b) {
+        DerivedArgs A{};
+        A.block = v->d_blocks + b;
+        A.cs = v->d_cases;
+        A.sgs = c->opts.sgs;
+        A.q = q[b];
+        A.out = out[b];
+        const BlockDev& B = v->hb[b];
+        CK(launch_derived(A, (long long)B.n[0] * B.n[1] * B.n[2], (cudaStream_t)stream));
+    }
     return WM_OK;
 }
 
