@@ -65,7 +65,7 @@ struct SurfaceArgs {
     GhostArgs G;
     WallArgs W;
     SpongeArgs S;          // nblocks = 0: no sponge
-    int g_ctas, w_per, w_ctas, s_per;
+    int g_ctas, w_per, w_ctas, s_per, s_ctas;
 };
 
 __device__ __forceinline__ long long cell_index(const BlockDev& B, int axis, int c, int a, int b) {

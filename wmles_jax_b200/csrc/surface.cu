@@ -290,22 +290,24 @@ cudaError_t launch_sponge_mean(const SpongeArgs& S, int max_rows, cudaStream_t s
 // ------------------------------------------------------------------ fused surface launch
 constexpr int SURF_NT = 256;
 
+// CTA order: wall faces first (the longest dependency chains: Newton iterations), then
+// sponge rows, then ghost entries, so the slow parts start in the first wave
 __global__ void __launch_bounds__(SURF_NT) surface_kernel(const __grid_constant__ SurfaceArgs A) {
     int bx = blockIdx.x;
-    if (bx < A.g_ctas) {
-        const int e = bx * SURF_NT + threadIdx.x;
-        if (e < A.G.total) ghost_entry(A.G, e);
-        return;
-    }
-    bx -= A.g_ctas;
     if (bx < A.w_ctas) {
         const int w = bx / A.w_per;
         wall_face(A.W, w, (long long)(bx - w * A.w_per) * SURF_NT + threadIdx.x);
         return;
     }
     bx -= A.w_ctas;
-    const int b = bx / A.s_per;
-    sponge_row(A.S, b, (bx - b * A.s_per) * (SURF_NT / 32) + (threadIdx.x >> 5), threadIdx.x & 31);
+    if (bx < A.s_ctas) {
+        const int b = bx / A.s_per;
+        sponge_row(A.S, b, (bx - b * A.s_per) * (SURF_NT / 32) + (threadIdx.x >> 5), threadIdx.x & 31);
+        return;
+    }
+    bx -= A.s_ctas;
+    const int e = bx * SURF_NT + threadIdx.x;
+    if (e < A.G.total) ghost_entry(A.G, e);
 }
 
 cudaError_t launch_surface(SurfaceArgs& A, int max_sponge_rows, cudaStream_t s) {
@@ -313,8 +315,8 @@ cudaError_t launch_surface(SurfaceArgs& A, int max_sponge_rows, cudaStream_t s) 
     A.w_per = A.W.nwalls ? (A.W.max_faces + SURF_NT - 1) / SURF_NT : 0;
     A.w_ctas = A.w_per * A.W.nwalls;
     A.s_per = A.S.nblocks ? (max_sponge_rows + SURF_NT / 32 - 1) / (SURF_NT / 32) : 0;
-    const int s_ctas = A.s_per * A.S.nblocks;
-    const int n = A.g_ctas + A.w_ctas + s_ctas;
+    A.s_ctas = A.s_per * A.S.nblocks;
+    const int n = A.g_ctas + A.w_ctas + A.s_ctas;
     if (n == 0) return cudaSuccess;
     surface_kernel<<<n, SURF_NT, 0, s>>>(A);
     return cudaGetLastError();
