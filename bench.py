@@ -344,7 +344,7 @@ def serving_leg(args):
             block_metrics(b, geo)
     reqs = serving_requests(n=args.serving_requests, rate=args.serving_rate, steps=args.serving_steps, seed=0)
     torch.cuda.synchronize()
-    srv = Server(precision="mixed", graphs=True, tile="auto", policy="sjf")
+    srv = Server(precision="mixed", graphs=True, tile="auto", policy="srpt")
     tile, tile_ms = srv.tune(reqs)              # before the arrivals start (cached per machine)
     srv.tile = tile
     results = srv.run(reqs, timeout=1800)
@@ -353,13 +353,15 @@ def serving_leg(args):
     return {"requests": st["requests"], "steps_per_request": args.serving_steps,
             "arrivals": f"Poisson, {args.serving_rate}/s, seed 0",
             "grids": [list(g) for g in SERVING_GRIDS], "re_tau": [550, 5200], "ma_b": [0.1, 0.5],
-            "form": "mixed", "admission": "shortest job first, 8M-cell resident budget, free-HBM check",
+            "form": "mixed", "scheduling": "least remaining work first within an 8M-cell step budget, "
+                                            "the rest paused on the device; cases built smallest first as "
+                                            "free HBM allows, up to twice the step budget ahead",
             "tile": tile, "tile_ms_per_step": tile_ms,
             "p50_time_to_result_s": st["p50_s"], "p99_time_to_result_s": st["p99_s"],
             "value": st["mcell_steps_per_s"], "unit": METRIC, "wall_s": st["wall_s"],
             "device_busy_s": st["device_busy_s"], "device_value": st["device_mcell_steps_per_s"],
             "cell_steps": st["cell_steps"], "batch_steps": st["batch_steps"], "graph_steps": st["graph_steps"],
-            "graph_captures": st["captures"], "memberships": st["memberships"],
+            "graph_captures": st["captures"], "memberships": st["memberships"], "pauses": st["pauses"],
             "gpu_launches": st["kernel_launches"], "peak_admitted_bytes": st["peak_admitted_bytes"],
             "nonfinite_results": bad,
             "time_to_result": "arrival to the host seeing the last step done on the device, including "

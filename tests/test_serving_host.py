@@ -3,7 +3,7 @@ estimate, the seeded request mix and the Re_tau -> Re_b mapping."""
 import numpy as np
 import pytest
 
-from wmles_jax_b200.serving import Admission, Request, estimate_bytes, pick_next
+from wmles_jax_b200.serving import Admission, Request, estimate_bytes, pick_next, select_active
 from wmles_jax_b200.workloads import SERVING_GRIDS, re_bulk_from_re_tau, serving_requests
 
 
@@ -89,3 +89,24 @@ def test_backend_names_the_drivers_use():
         assert backend.DEVICE is None
         with pytest.raises(RuntimeError):
             backend.asarray([1.0, 2.0])
+
+
+class _Res:
+    def __init__(self, req, done=0):
+        self.req, self.done = req, done
+
+
+def test_select_active_least_remaining_work_within_budget():
+    a = _Res(_req(0, (40, 40, 40), 100, 0.0))            # 64000 cells, 6.4 M cell-steps
+    b = _Res(_req(1, (8, 8, 8), 100, 0.5))               # 512 cells
+    c = _Res(_req(2, (20, 20, 20), 100, 0.2), done=50)   # 8000 cells, half done
+    assert [r.req.rid for r in select_active([a, b, c], "srpt", None)] == [1, 2, 0]
+    # a budget that does not hold the big case pauses it; the first case is always taken
+    assert [r.req.rid for r in select_active([a, b, c], "srpt", 10000)] == [1, 2]
+    assert [r.req.rid for r in select_active([a], "srpt", 10)] == [0]
+    # remaining work, not size: the big case near its end (64000 cell-steps left) overtakes
+    # the half-done medium one (400000 left)
+    a.done = 99
+    assert [r.req.rid for r in select_active([a, b, c], "srpt", None)] == [1, 0, 2]
+    assert [r.req.rid for r in select_active([a, b, c], "fifo", None)] == [0, 2, 1]
+    assert len(select_active([_Res(_req(i, (4, 4, 4), 1, 0.0)) for i in range(200)], "srpt", None)) == 96

@@ -13,9 +13,10 @@ waiting ones, so requests that arrive while others run join the next step.
 * Admission: a request is admitted when its estimated device bytes fit in the free HBM
   (device free memory plus what PyTorch's allocator holds unused) minus a reserve, and the
   batch has block slots left (at most ``WM_MAX_BLOCKS`` blocks per batch).
-* Admission order is shortest-job-first (least cells x steps) among arrived requests, or
-  FIFO; a cell budget caps the resident set at a few GPU-fulls of cells, so short requests
-  do not wait behind long ones while the GPU stays full.
+* Scheduling: every resident case is a candidate each time the set changes (an arrival or
+  a completion); the cases with the least remaining work (cells x steps left) are stepped,
+  up to a cell budget that fills the GPU, and the others stay paused on the device, so
+  short requests do not wait behind long ones while the GPU stays full (FIFO available).
 * Host preparation (lowering, ghost programs, initial state) runs on builder threads,
   overlapping the GPU steps; graph captures and device-side case construction exclude each
   other.
@@ -207,6 +208,28 @@ class Result:
         return self.finished - self.arrival
 
 
+def select_active(resident, policy, max_cells, max_blocks=N.MAX_BLOCKS):
+    """Resident cases to step next: in policy order ("srpt": least remaining work, cells x
+    steps left, first; "fifo": arrival order), taken greedily while the batch stays within
+    `max_cells` interior cells (None: no limit) and `max_blocks` blocks and cases (the first
+    case always).  The others stay resident and paused.  Items need ``.req`` (a Request)
+    and ``.done`` (steps taken)."""
+    if policy == "fifo":
+        order = sorted(resident, key=lambda r: (r.req.arrival, r.req.rid))
+    else:
+        order = sorted(resident, key=lambda r: (r.req.cells * (r.req.steps - r.done), r.req.arrival, r.req.rid))
+    chosen, cells, blocks = [], 0, 0
+    for r in order:
+        nb = len(r.req.dims)
+        if chosen and (blocks + nb > max_blocks or len(chosen) + 1 > max_blocks
+                       or (max_cells is not None and cells + r.req.cells > max_cells)):
+            continue
+        chosen.append(r)
+        cells += r.req.cells
+        blocks += nb
+    return chosen
+
+
 # ---------------------------------------------------------------------------- server
 class Server:
     """Continuous-batching server (see the module docstring).
@@ -214,22 +237,29 @@ class Server:
     precision / tile / chunk: solver options shared by every case (one batch; tile="auto" tunes
     the tile shape over the grids of the requests before serving); graphs: replay
     steps from CUDA graphs once a membership has run ``graph_after`` steps eagerly;
-    reserve_bytes: HBM left free; budget_bytes: override of the admission budget; max_cells:
-    interior-cell budget of the resident set; policy: admission order ("sjf" or "fifo");
-    builders: host threads preparing admitted cases."""
+    reserve_bytes: HBM left free; budget_bytes: override of the memory budget of built cases;
+    max_cells: interior cells stepped together (None: all resident cases); policy: which
+    resident cases are stepped ("srpt": least remaining work first, the others paused on the
+    device until they are among the least again; "fifo": arrival order); builders: host
+    threads preparing cases (smallest first, or in arrival order under "fifo")."""
 
     def __init__(self, precision="mixed", tile=None, chunk=None, graphs=True, graph_after=2,
-                 reserve_bytes=4 << 30, budget_bytes=None, max_cells=8 << 20, policy="sjf", builders=2,
+                 reserve_bytes=4 << 30, budget_bytes=None, max_cells=8 << 20, policy="srpt", builders=2,
                  device=None):
         from .backend import require_gpu
         self.device = device or require_gpu()
         self.precision, self.tile, self.chunk = precision, tile, chunk
         self.tuned = None
         self.graphs, self.graph_after = graphs, graph_after
-        order_key(policy)
+        if policy not in ("srpt", "fifo"):
+            raise ValueError(f"unknown scheduling policy {policy!r}")
         self.policy, self.builders = policy, max(1, int(builders))
+        self.max_cells = max_cells
         budget = budget_bytes if budget_bytes is not None else free_device_bytes(self.device) - reserve_bytes
-        self.admission = Admission(max(0, budget), max_cells=max_cells)
+        # building is bounded by memory and by a lookahead of twice the cell budget (built,
+        # unfinished cases); the cell budget bounds the cases stepped together
+        self.admission = Admission(max(0, budget), max_blocks=1 << 30, max_cases=1 << 30,
+                                   max_cells=None if max_cells is None else 2 * max_cells)
         self.stream = torch.cuda.Stream(self.device)
         self._lock = threading.Lock()             # case construction vs graph capture
         self._cond = threading.Condition()        # admission waits for retirements
@@ -268,7 +298,8 @@ class Server:
                             return
                         now = time.perf_counter() - t0
                         waiting = [r for r in todo if r.arrival <= now]
-                        req = pick_next(waiting, self.admission, self.precision, self.policy)
+                        req = pick_next(waiting, self.admission, self.precision,
+                                        "fifo" if self.policy == "fifo" else "sjf")
                         if req is not None:
                             break
                         nxt = min(r.arrival for r in todo) - now
@@ -317,6 +348,9 @@ class Server:
         finally:
             self._lock.release()
 
+    def _select(self, resident):
+        return select_active(resident, self.policy, self.max_cells)
+
     def run(self, requests, timeout=None):
         """Serve ``requests`` (arrival times relative to now); returns {rid: Result}."""
         if self.tile == "auto":
@@ -329,11 +363,12 @@ class Server:
                    for _ in range(self.builders)]
         for w in workers:
             w.start()
-        active, joined, results = [], [], {}
+        resident, active, joined, results = [], [], [], {}
         pending = []               # (event, [residents finished by that step]) of steps in flight
         batch, args, graphs, run_len = None, {}, {}, 0
         builder_done = False
-        n = dict(batch_steps=0, graph_steps=0, captures=0, memberships=0, kernel_launches=0, cell_steps=0)
+        n = dict(batch_steps=0, graph_steps=0, captures=0, memberships=0, kernel_launches=0, cell_steps=0,
+                 pauses=0)
         seg, busy_ms = None, 0.0    # device time of the batch steps, per membership segment
 
         def close_segment():
@@ -379,7 +414,7 @@ class Server:
                     raise errors[0]
                 if timeout is not None and clock() > timeout:
                     raise TimeoutError("serving did not finish in time")
-                if not active and not joined and not builder_done:
+                if not resident and not joined and not builder_done:
                     try:                       # idle: wait for the next admitted case
                         take(ready.get(timeout=0.05))
                     except queue.Empty:
@@ -390,34 +425,38 @@ class Server:
                     except queue.Empty:
                         break
                 leaving = [r for r in active if r.done >= r.req.steps]
-                if joined or leaving or (batch is None and active):
-                    # membership change: drain the steps in flight, free the leavers, rebuild
-                    close_segment()
-                    self.stream.synchronize()
-                    stamp(0)
-                    graphs.clear()
-                    args = {}
-                    if batch is not None:
-                        batch.close()
-                        batch = None
-                    active = [r for r in active if r.done < r.req.steps]
-                    release(leaving)
+                if joined or leaving or (batch is None and resident):
                     for r in joined:
                         if r.req.steps <= 0:
                             results[r.req.rid] = Result(r.req.rid, r.bufs[0], r.dts[0], 0, r.req.cells,
                                                         r.req.arrival, r.admitted, clock())
                             release([r])
                         else:
-                            active.append(r)
+                            resident.append(r)
                     joined = []
-                    if active:
-                        batch = Batch([r.solver for r in active])
-                        n["memberships"] += 1
-                        run_len = 0
-                        seg = torch.cuda.Event(enable_timing=True)
-                        seg.record(self.stream)
+                    resident = [r for r in resident if r.done < r.req.steps]
+                    chosen = self._select(resident)
+                    if leaving or [id(r) for r in chosen] != [id(r) for r in active]:
+                        # membership change: drain the steps in flight, free the leavers, rebuild
+                        close_segment()
+                        self.stream.synchronize()
+                        stamp(0)
+                        graphs.clear()
+                        args = {}
+                        if batch is not None:
+                            batch.close()
+                            batch = None
+                        release(leaving)
+                        n["pauses"] += sum(1 for r in active if r.done < r.req.steps and r not in chosen)
+                        active = chosen
+                        if active:
+                            batch = Batch([r.solver for r in active])
+                            n["memberships"] += 1
+                            run_len = 0
+                            seg = torch.cuda.Event(enable_timing=True)
+                            seg.record(self.stream)
                 if not active:
-                    if builder_done and ready.empty():
+                    if builder_done and ready.empty() and not resident:
                         break
                     continue
                 key = tuple(r.parity for r in active)
