@@ -202,6 +202,41 @@ int upload_prog(wm_case* c, GhostProg* g, const wm_ghost_program& p) {
     return WM_OK;
 }
 
+// every index of a ghost-cell program inside its arrays: the gather kernel trusts them
+int validate_program(const wm_case_desc* d, const wm_ghost_program& p, const char* name) {
+    if (p.count < 0 || p.nops < 0) return fail(WM_E_INVALID, "%s: negative count", name);
+    if (p.count > 0 && (!p.dst || !p.src || !p.ops)) return fail(WM_E_INVALID, "%s: null arrays", name);
+    if (p.nops > 0 && (!p.op_code || !p.op_nrm)) return fail(WM_E_INVALID, "%s: null op arrays", name);
+    auto cells = [&](int b) {
+        const wm_block& B = d->blocks[b];
+        return (long long)(B.n[0] + 2 * B.ng) * (B.n[1] + 2 * B.ng) * (B.n[2] + 2 * B.ng);
+    };
+    long long inflow_n = 0;
+    if (d->inflow) {
+        const wm_block& B = d->blocks[d->inflow->block];
+        inflow_n = (long long)B.ng * (B.n[1] + 2 * B.ng) * (B.n[2] + 2 * B.ng);
+    }
+    for (int e = 0; e < p.count; ++e) {
+        const int db = p.dst[2 * e], dc = p.dst[2 * e + 1];
+        if (db < 0 || db >= d->nblocks || dc < 0 || dc >= cells(db))
+            return fail(WM_E_INVALID, "%s entry %d: destination out of range", name, e);
+        const int kind = p.src[2 * e] >> 24, sb = p.src[2 * e] & 0xffffff, sc = p.src[2 * e + 1];
+        const bool ok = kind == WM_SRC_CELL ? (sb < d->nblocks && sc >= 0 && sc < cells(sb))
+                        : kind == WM_SRC_INFLOW ? (d->inflow && sc >= 0 && sc < inflow_n)
+                        : kind == WM_SRC_CONST ? (sb < d->nbc) : false;
+        if (!ok) return fail(WM_E_INVALID, "%s entry %d: source out of range", name, e);
+        const int o0 = p.ops[2 * e], no = p.ops[2 * e + 1];
+        if (o0 < 0 || no < 0 || (long long)o0 + no > p.nops)
+            return fail(WM_E_INVALID, "%s entry %d: map chain out of range", name, e);
+    }
+    for (int o = 0; o < p.nops; ++o) {
+        const int code = p.op_code[o] & 0xff, bc = (p.op_code[o] >> 8) & 0xff;
+        if (code < WM_OP_SLIP || code > WM_OP_FARFIELD || ((code != WM_OP_SLIP) && bc >= d->nbc))
+            return fail(WM_E_INVALID, "%s map %d: bad code or BC id", name, o);
+    }
+    return WM_OK;
+}
+
 int validate(const wm_case_desc* d) {
     if (!d) return fail(WM_E_INVALID, "null descriptor");
     if (d->nblocks < 1 || d->nblocks > WM_MAX_BLOCKS)
@@ -229,6 +264,25 @@ int validate(const wm_case_desc* d) {
         if (W.n_match < 1 || W.n_match > n) return fail(WM_E_INVALID, "wall %d: n_match=%d", w, W.n_match);
     }
     if (d->cmf_dir >= 0 && !(d->cmf_volume > 0)) return fail(WM_E_INVALID, "cmf_volume must be positive");
+    if (d->cmf_dir > 2) return fail(WM_E_INVALID, "cmf_dir=%d", d->cmf_dir);
+    if (!(d->cfl > 0)) return fail(WM_E_INVALID, "cfl must be positive");
+    for (int w = 0; w < d->nwalls; ++w) {
+        const wm_wall& W = d->walls[w];
+        if (!W.geom) return fail(WM_E_INVALID, "wall %d: null geometry", w);
+        if (W.n_iter < 0 || W.n_iter > 1000) return fail(WM_E_INVALID, "wall %d: n_iter=%d", w, W.n_iter);
+    }
+    if (d->nbc < 0 || (d->nbc > 0 && !d->bc_table)) return fail(WM_E_INVALID, "bad BC table");
+    if (d->inflow) {
+        const wm_inflow& I = *d->inflow;
+        if (I.block < 0 || I.block >= d->nblocks) return fail(WM_E_INVALID, "inflow block %d", I.block);
+        if (I.n_modes < 1 || I.n_tab < 2 || !I.modes || !I.table) return fail(WM_E_INVALID, "bad inflow tables");
+        if (!(I.L > 0)) return fail(WM_E_INVALID, "inflow length scale must be positive");
+    }
+    if (d->sponge.enabled && !(d->sponge.x_end_l > d->sponge.x_start_l && d->sponge.L > 0))
+        return fail(WM_E_INVALID, "bad sponge extent");
+    int r;
+    if ((r = validate_program(d, d->ghost_rhs, "ghost_rhs"))) return r;
+    if ((r = validate_program(d, d->ghost_all, "ghost_all"))) return r;
     return WM_OK;
 }
 
