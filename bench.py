@@ -363,7 +363,7 @@ def serving_leg(args):
             "cell_steps": st["cell_steps"], "batch_steps": st["batch_steps"], "graph_steps": st["graph_steps"],
             "graph_captures": st["captures"], "memberships": st["memberships"], "pauses": st["pauses"],
             "gpu_launches": st["kernel_launches"], "peak_admitted_bytes": st["peak_admitted_bytes"],
-            "nonfinite_results": bad,
+            "nonfinite_results": bad, "failed_requests": st["failed"],
             "time_to_result": "arrival to the host seeing the last step done on the device, including "
                               "host-side case preparation (IC, ghost programs) and admission"}
 

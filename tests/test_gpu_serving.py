@@ -126,3 +126,19 @@ def test_autotune_picks_a_measured_tile(tmp_path, monkeypatch):
     assert all(v > 0 for v in ms.values())
     tile2, ms2 = autotune.tune(cases, precision="mixed")     # served from the cache
     assert tile2 == tile and ms2 == ms
+
+
+def test_server_survives_a_failing_request():
+    """A request whose case cannot be built fails alone; the others are served unchanged."""
+    from wmles_jax_b200.serving import Request, Server, serve_alone
+
+    def bad():
+        raise ValueError("no such grid")
+    reqs = _requests([6, 4], [0.0, 0.1])
+    reqs.append(Request(rid=99, build=bad, steps=5, arrival=0.05, dims=((8, 8, 8),)))
+    alone = [serve_alone(r) for r in reqs[:2]]
+    srv = Server(precision="mixed", graphs=False)
+    results = srv.run(reqs, timeout=300)
+    assert not results[99].ok and "no such grid" in results[99].error
+    _check_server({k: v for k, v in results.items() if k != 99}, reqs[:2], alone)
+    assert srv.stats["failed"] == 1 and srv.stats["nonfinite"] == 0

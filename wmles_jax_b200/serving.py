@@ -195,13 +195,18 @@ class _Resident:
 @dataclass
 class Result:
     rid: int
-    state: tuple          # final state (device tensors)
-    dt: torch.Tensor      # CFL time step of the final state (device)
+    state: tuple          # final state (device tensors); None if the request failed
+    dt: torch.Tensor      # CFL time step of the final state (device); NaN if the state is not finite
     steps: int
     cells: int
     arrival: float
     admitted: float
     finished: float
+    error: str = None     # why the request could not be served (its case could not be built)
+
+    @property
+    def ok(self):
+        return self.error is None
 
     @property
     def time_to_result(self):
@@ -307,7 +312,15 @@ class Server:
                     todo.remove(req)
                     nbytes = estimate_bytes(req.dims, self.precision)
                     self.admission.take(nbytes, len(req.dims), req.cells)
-                solver, bufs, dts = self._build(req, bstream)
+                try:
+                    solver, bufs, dts = self._build(req, bstream)
+                except Exception as e:      # this request fails; the server goes on
+                    with self._cond:
+                        self.admission.give(nbytes, len(req.dims), req.cells)
+                        self._cond.notify_all()
+                    ready.put(Result(req.rid, None, None, 0, req.cells, req.arrival, time.perf_counter() - t0,
+                                     time.perf_counter() - t0, error=f"{type(e).__name__}: {e}"))
+                    continue
                 ready.put(_Resident(req, solver, bufs, dts, nbytes, admitted=time.perf_counter() - t0))
         except BaseException as e:   # surfaced by run()
             errors.append(e)
@@ -387,6 +400,8 @@ class Server:
             nonlocal builder_done
             if item is None:
                 builder_done = True
+            elif isinstance(item, Result):      # a request that failed to build
+                results[item.rid] = item
             else:
                 joined.append(item)
 
@@ -499,9 +514,12 @@ class Server:
             w.join()
         if errors:
             raise errors[0]
-        wall = max((r.finished for r in results.values()), default=0.0)
-        ttr = np.array([r.time_to_result for r in results.values()])
-        self.stats = dict(n, requests=len(results), wall_s=wall, peak_admitted_bytes=self.admission.peak,
+        served = [r for r in results.values() if r.ok]
+        wall = max((r.finished for r in served), default=0.0)
+        ttr = np.array([r.time_to_result for r in served])
+        nonfinite = sum(1 for r in served if not np.isfinite(float(r.dt)))
+        self.stats = dict(n, requests=len(results), failed=len(results) - len(served), nonfinite=nonfinite,
+                          wall_s=wall, peak_admitted_bytes=self.admission.peak,
                           mcell_steps_per_s=n["cell_steps"] / wall / 1e6 if wall > 0 else 0.0,
                           device_busy_s=busy_ms * 1e-3,
                           device_mcell_steps_per_s=n["cell_steps"] / (busy_ms * 1e-3) / 1e6 if busy_ms > 0 else 0.0,
