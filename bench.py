@@ -398,7 +398,10 @@ def run_reference(args, rank, world):
         return None
     import multiprocessing as mp
     workers = max(1, min(os.cpu_count() or 1, args.max_workers))
-    n = (args.cpu_cells, N_CFG2[1], N_CFG2[2])
+    # each step is one oracle step on a slab of the workload (~1.6 s on an 8-cell slab per
+    # core); long runs use a 4-cell slab so that the whole run stays within a few minutes
+    nx = args.cpu_cells if args.steps + args.warmup <= 100 else max(4, args.cpu_cells // 2)
+    n = (nx, N_CFG2[1], N_CFG2[2])
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(workers) as pool:
