@@ -7,7 +7,7 @@
 // single-case entry points; a wm_batch is a View over several resident cases, so one
 // launch per kernel and stage advances all of them.  The stage work list is cut for the
 // whole view (longer chunks along i when many cases share the GPU).  Per-case reductions
-// (CFL minimum; constant-mass-flux sum over fixed per-column, per-plane, per-warp partials)
+// (CFL minimum; constant-mass-flux sum over fixed per-column, per-plane partials)
 // run in a fixed order, so a case's result depends neither on the chunk length nor on what
 // else is in the batch.
 #include <algorithm>
@@ -313,12 +313,11 @@ int choose_chunk(const std::vector<BlockDev>& hb, const StageOpts& opts, int tj,
 }
 
 // stage work list of a view: every (j,k) column of every block, cut into chunks of ic planes;
-// plus the constant-mass-flux partial slots, one per (column, interior plane, warp) of each
+// plus the constant-mass-flux partial slots, one per (column, interior plane) of each
 // block, which do not depend on ic
 void build_tiles(View* v, int tj, int tk, int ic) {
     v->tiles.clear();
     v->cmf_slot_start.assign(1, 0);
-    const int warps = tj * tk / 32;
     for (int b = 0; b < v->nblocks; ++b) {
         const BlockDev& B = v->hb[b];
         const int ng = B.ng;
@@ -327,7 +326,7 @@ void build_tiles(View* v, int tj, int tk, int ic) {
                 for (int k0 = ng; k0 < ng + B.n[2]; k0 += tk)
                     v->tiles.push_back(Tile{b, j0, k0, i0, std::min(i0 + ic, ng + B.n[0])});
         const int cols = ((B.n[1] + tj - 1) / tj) * ((B.n[2] + tk - 1) / tk);
-        v->cmf_slot_start.push_back(v->cmf_slot_start.back() + cols * B.n[0] * warps);
+        v->cmf_slot_start.push_back(v->cmf_slot_start.back() + cols * B.n[0]);
     }
     v->case_slot_start.clear();
     for (int c = 0; c <= v->ncases; ++c) v->case_slot_start.push_back(v->cmf_slot_start[v->case_block_start[c]]);

@@ -16,7 +16,7 @@
 //   3. own i-face flux -> RK epilogue of plane i-1; all j/k faces of plane i (flat loop);
 //      the cp.async of plane i+2 is in flight meanwhile
 // Each face flux is evaluated once; each conservative value is read from HBM about once
-// per stage (halo re-reads hit L2).  Stage 3 also emits per-tile partial sums of
+// per stage (halo re-reads hit L2).  Stage 3 also emits per-(column, plane) partial sums of
 // rho u V for the constant-mass-flux constraint.
 //
 // Reference: Solver._block_rhs (wmles/solver.py:76-95), green_gauss / viscous_flux /
@@ -372,15 +372,16 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
 
     const int i0 = t.i0, i1 = t.i1;
     const double dt = A.stage ? *A.dt[B.case_id] : 0.0;
-    // constant mass flux (stage 3): one partial of rho u_dir V per (tile column, plane, warp),
-    // so the case's sum does not depend on how the columns are cut into chunks along i
+    // constant mass flux (stage 3): one partial of rho u_dir V per (tile column, plane) -
+    // the warps' sums of the plane added in warp order in shared memory - so the case's sum
+    // does not depend on how the columns are cut into chunks along i
     const bool cmf_on = A.stage == 3 && A.cmf_part != nullptr && C.cmf_dir >= 0;
     double cmf_acc = 0.0;
     double* cmf_col = nullptr;
     if (cmf_on) {
         const int ncolk = (B.n[2] + TK - 1) / TK;
         const int col = ((t.j0 - ng) / TJ) * ncolk + (t.k0 - ng) / TK;
-        cmf_col = A.cmf_part + A.cmf_slot_start[t.blk] + (long long)col * B.n[0] * (NT / 32) + (tid >> 5);
+        cmf_col = A.cmf_part + A.cmf_slot_start[t.blk] + (long long)col * B.n[0];
     }
 
     // ---- RK epilogue of interior cell (io, j, k): r = -(div F)/V (+ source), stage update
@@ -469,13 +470,19 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
         if (cmf_on) {
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) cmf_acc += __shfl_down_sync(0xffffffffu, cmf_acc, off);
-            if ((tid & 31) == 0) cmf_col[(ip - 1 - ng) * (NT / 32)] = cmf_acc;
+            // warp sums of this plane; two buffers by plane parity (read after the barrier below)
+            if ((tid & 31) == 0) red[(ip & 1) * (NT / 32) + (tid >> 5)] = cmf_acc;
             cmf_acc = 0.0;
         }
         if (ip < i1)
             for (int f = tid; f < LY::FJN + LY::FKN; f += NT) jk_face(ip, f);
         cp_async_wait_all();
         __syncthreads();
+        if (cmf_on && tid == 0) {
+            double sp = 0.0;
+            for (int w = 0; w < NT / 32; ++w) sp += red[(ip & 1) * (NT / 32) + w];
+            cmf_col[ip - 1 - ng] = sp;
+        }
         if (ip < i1) {
             jk_diff();
             save_gs();
@@ -485,7 +492,7 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
     if (A.stage == 3 && A.cmf_part != nullptr) {
         // every CTA of the launch signals; the last one reduces each case's partials
         __shared__ bool last;
-        if (cmf_on && (tid & 31) == 0) __threadfence();
+        if (cmf_on && tid == 0) __threadfence();
         __syncthreads();
         if (tid == 0) last = atomicAdd(A.cmf_counter, 1u) == unsigned(gridDim.x - 1);
         __syncthreads();
