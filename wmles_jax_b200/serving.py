@@ -24,13 +24,14 @@ waiting ones, so requests that arrive while others run join the next step.
   a fixed order and its stage tiles are fixed at construction, so a case advanced in any
   batch is bit-identical to the same case advanced alone with ``Solver.step``.
 * Time-to-result is measured from the request's arrival to the moment the host sees the
-  device finish the request's last step (an event per step, at most two steps in flight).
+  device finish the request's last step (an event per step, at most six steps in flight).
 
 No reference counterpart: the reference advances one case per ``Solver`` in a Python loop
 (examples/channel_wmles.py:121-152).
 """
 import ctypes as C
 import queue
+import sys
 import threading
 import time
 from dataclasses import dataclass, field
@@ -256,6 +257,7 @@ class Server:
         self.precision, self.tile, self.chunk = precision, tile, chunk
         self.tuned = None
         self.graphs, self.graph_after = graphs, graph_after
+        self.in_flight = 6          # steps queued ahead: slack against host-side stalls
         if policy not in ("srpt", "fifo"):
             raise ValueError(f"unknown scheduling policy {policy!r}")
         self.policy, self.builders = policy, max(1, int(builders))
@@ -371,6 +373,16 @@ class Server:
             self.tile = self.tuned[0]
         todo = sorted(requests, key=lambda r: r.arrival)
         ready, errors, left = queue.Queue(), [], [self.builders]
+        # hand the interpreter lock over often: the builder threads run Python-heavy host
+        # preparation while this thread must keep the device queue fed
+        switch = sys.getswitchinterval()
+        sys.setswitchinterval(5e-4)
+        try:
+            return self._run(todo, ready, errors, left, timeout)
+        finally:
+            sys.setswitchinterval(switch)
+
+    def _run(self, todo, ready, errors, left, timeout):
         t0 = time.perf_counter()
         workers = [threading.Thread(target=self._builder, args=(todo, t0, ready, errors, left), daemon=True)
                    for _ in range(self.builders)]
@@ -504,7 +516,7 @@ class Server:
                 ev = torch.cuda.Event()
                 ev.record(self.stream)
                 pending.append((ev, fin))
-                stamp(2)                       # at most two steps in flight
+                stamp(self.in_flight)          # bounded number of steps in flight
             close_segment()
             self.stream.synchronize()
             stamp(0)
