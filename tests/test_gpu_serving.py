@@ -136,9 +136,11 @@ def test_server_survives_a_failing_request():
         raise ValueError("no such grid")
     reqs = _requests([6, 4], [0.0, 0.1])
     reqs.append(Request(rid=99, build=bad, steps=5, arrival=0.05, dims=((8, 8, 8),)))
+    reqs.append(Request(rid=98, build=bad, steps=5, arrival=0.0, dims=((4096, 4096, 4096),)))
     alone = [serve_alone(r) for r in reqs[:2]]
     srv = Server(precision="mixed", graphs=False)
     results = srv.run(reqs, timeout=300)
     assert not results[99].ok and "no such grid" in results[99].error
-    _check_server({k: v for k, v in results.items() if k != 99}, reqs[:2], alone)
-    assert srv.stats["failed"] == 1 and srv.stats["nonfinite"] == 0
+    assert not results[98].ok and "memory" in results[98].error
+    _check_server({k: v for k, v in results.items() if k not in (98, 99)}, reqs[:2], alone)
+    assert srv.stats["failed"] == 2 and srv.stats["nonfinite"] == 0

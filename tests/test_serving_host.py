@@ -17,6 +17,7 @@ def test_admission_accounting():
     assert not a.fits(0, 1)            # blocks and cases
     a.give(600, 1)
     assert a.fits(500, 1) and a.peak == 1000 and a.used == 400
+    assert a.never_fits(2000, 1) and not a.never_fits(1000, 1)
     with pytest.raises(ValueError):
         a.fits(2000, 1)                # can never be admitted
     with pytest.raises(ValueError):

@@ -138,6 +138,10 @@ class Admission:
         self.cells = 0
         self.peak = 0             # most bytes ever charged at once
 
+    def never_fits(self, nbytes, nblocks):
+        """True for a request that exceeds the limits even with nothing else admitted."""
+        return nbytes > self.budget or nblocks > self.max_blocks
+
     def fits(self, nbytes, nblocks, ncells=0):
         if nbytes > self.budget or nblocks > self.max_blocks:
             raise ValueError(f"request needs {nbytes} bytes / {nblocks} blocks: it can never be admitted "
@@ -305,6 +309,12 @@ class Server:
                             return
                         now = time.perf_counter() - t0
                         waiting = [r for r in todo if r.arrival <= now]
+                        for r in [r for r in waiting if self.admission.never_fits(
+                                estimate_bytes(r.dims, self.precision), len(r.dims))]:
+                            todo.remove(r)     # larger than the whole budget: fails alone
+                            waiting.remove(r)
+                            ready.put(Result(r.rid, None, None, 0, r.cells, r.arrival, now, now,
+                                             error="MemoryError: larger than the device memory budget"))
                         req = pick_next(waiting, self.admission, self.precision,
                                         "fifo" if self.policy == "fifo" else "sjf")
                         if req is not None:
