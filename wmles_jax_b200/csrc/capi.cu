@@ -539,7 +539,15 @@ int wm_case_create(const wm_case_desc* d, wm_case** out) {
     if (r) return r;
     wm_case* c = new wm_case();
     auto bail = [&](int code) { delete c; return code; };
-    CK(cudaGetDevice(&c->device));
+    // a failed CUDA call frees the partly built case (its allocations are owned by it)
+#define CKB(call)                                                                            \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return bail(fail(WM_E_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                             __FILE__, __LINE__));                                           \
+    } while (0)
+    CKB(cudaGetDevice(&c->device));
 
     // ---- physical constants
     const wm_gas& g = d->gas;
@@ -595,7 +603,7 @@ int wm_case_create(const wm_case_desc* d, wm_case** out) {
         for (int s = 0; s < 2; ++s) {
             double* w = nullptr;
             if ((r = c->mem.alloc(&w, 5 * (size_t)B.ncell))) return bail(r);
-            CK(cudaMemset(w, 0, sizeof(double) * 5 * B.ncell));
+            CKB(cudaMemset(w, 0, sizeof(double) * 5 * B.ncell));
             c->work[s].push_back(w);
         }
     }
@@ -657,14 +665,15 @@ int wm_case_create(const wm_case_desc* d, wm_case** out) {
     for (const BlockDev& B : c->hb) max_nj = std::max(max_nj, B.n[1]);
     if ((r = c->mem.alloc(&c->ps_part, (size_t)PS_NQ * max_nj * PS_CHUNKS))) return bail(r);
     if ((r = c->mem.alloc(&c->ps_counter, 1))) return bail(r);
-    CK(cudaMemset(c->ps_counter, 0, sizeof(unsigned)));
+    CKB(cudaMemset(c->ps_counter, 0, sizeof(unsigned)));
 
     c->self = new View();
     wm_case* self_list[1] = {c};
     if ((r = build_view(c->self, self_list, 1))) return bail(r);
-    CK(cudaDeviceSynchronize());
+    CKB(cudaDeviceSynchronize());
     *out = c;
     return WM_OK;
+#undef CKB
 }
 
 int wm_apply_bcs(wm_case* c, double* const* q, double time, void* stream) {
