@@ -519,6 +519,17 @@ int run_step(View* v, Prof* pf, double* const* q_in, double* const* q_out, doubl
 
 wm_case::~wm_case() { delete self; }
 
+namespace {
+// every per-block (or per-case) pointer of an argument array is set: a null one would
+// become a device fault
+int check_ptrs(const void* const* p, int n, const char* what) {
+    if (!p) return fail(WM_E_INVALID, "null %s array", what);
+    for (int i = 0; i < n; ++i)
+        if (!p[i]) return fail(WM_E_INVALID, "null %s[%d]", what, i);
+    return WM_OK;
+}
+}  // namespace
+
 struct wm_batch {
     View view;
     Prof prof;
@@ -677,7 +688,8 @@ int wm_case_create(const wm_case_desc* d, wm_case** out) {
 }
 
 int wm_apply_bcs(wm_case* c, double* const* q, double time, void* stream) {
-    if (!c || !q) return fail(WM_E_INVALID, "null argument");
+    if (!c) return fail(WM_E_INVALID, "null case");
+    if (int r = check_ptrs((const void* const*)q, c->self->nblocks, "q")) return r;
     cudaStream_t s = (cudaStream_t)stream;
     View* v = c->self;
     int r;
@@ -691,18 +703,23 @@ int wm_apply_bcs(wm_case* c, double* const* q, double time, void* stream) {
 }
 
 int wm_rhs(wm_case* c, double* const* q, double* const* rr, double time, void* stream) {
-    if (!c || !q || !rr) return fail(WM_E_INVALID, "null argument");
+    if (!c) return fail(WM_E_INVALID, "null case");
+    if (int r = check_ptrs((const void* const*)q, c->self->nblocks, "q")) return r;
+    if (int r = check_ptrs((const void* const*)rr, c->self->nblocks, "r")) return r;
     return run_stage(c->self, &c->prof, 0, q, nullptr, rr, nullptr, &time, 0.0, (cudaStream_t)stream);
 }
 
 int wm_max_dt(wm_case* c, const double* const* q, double* dt_dev, void* stream) {
-    if (!c || !q || !dt_dev) return fail(WM_E_INVALID, "null argument");
+    if (!c || !dt_dev) return fail(WM_E_INVALID, "null argument");
+    if (int r = check_ptrs((const void* const*)q, c->self->nblocks, "q")) return r;
     return run_dt(c->self, &c->prof, const_cast<double* const*>(q), false, true, &dt_dev, (cudaStream_t)stream);
 }
 
 int wm_advance(wm_case* c, double* const* q_in, double* const* q_out, const double* dt_dev, double time,
                void* stream) {
-    if (!c || !q_in || !q_out || !dt_dev) return fail(WM_E_INVALID, "null argument");
+    if (!c || !dt_dev) return fail(WM_E_INVALID, "null argument");
+    if (int r = check_ptrs((const void* const*)q_in, c->self->nblocks, "q_in")) return r;
+    if (int r = check_ptrs((const void* const*)q_out, c->self->nblocks, "q_out")) return r;
     return run_step(c->self, &c->prof, q_in, q_out, c->work[0].data(), c->work[1].data(), &dt_dev, nullptr, &time,
                     false, (cudaStream_t)stream);
 }
@@ -715,13 +732,17 @@ int wm_step(wm_case* c, double* const* q_in, double* const* q_out, double* dt_de
 
 int wm_step_fused(wm_case* c, double* const* q_in, double* const* q_out, const double* dt_in, double* dt_next,
                   double time, void* stream) {
-    if (!c || !q_in || !q_out || !dt_in || !dt_next) return fail(WM_E_INVALID, "null argument");
+    if (!c || !dt_in || !dt_next) return fail(WM_E_INVALID, "null argument");
+    if (int r = check_ptrs((const void* const*)q_in, c->self->nblocks, "q_in")) return r;
+    if (int r = check_ptrs((const void* const*)q_out, c->self->nblocks, "q_out")) return r;
     return run_step(c->self, &c->prof, q_in, q_out, c->work[0].data(), c->work[1].data(), &dt_in, &dt_next, &time,
                     true, (cudaStream_t)stream);
 }
 
 int wm_wall_stats(wm_case* c, const double* const* q, double* const* out, void* stream) {
-    if (!c || !q || !out) return fail(WM_E_INVALID, "null argument");
+    if (!c) return fail(WM_E_INVALID, "null case");
+    if (int r = check_ptrs((const void* const*)q, c->self->nblocks, "q")) return r;
+    if (int r = check_ptrs((const void* const*)out, (int)c->self->hw.size(), "out")) return r;
     cudaStream_t s = (cudaStream_t)stream;
     View* v = c->self;
     if (v->hw.empty()) return WM_OK;
@@ -757,7 +778,9 @@ int wm_plane_stats(wm_case* c, int block, const double* q, double* sum, void* st
 }
 
 int wm_derived_fields(wm_case* c, const double* const* q, double* const* out, void* stream) {
-    if (!c || !q || !out) return fail(WM_E_INVALID, "null argument");
+    if (!c) return fail(WM_E_INVALID, "null case");
+    if (int r = check_ptrs((const void* const*)q, c->self->nblocks, "q")) return r;
+    if (int r = check_ptrs((const void* const*)out, c->self->nblocks, "out")) return r;
     View* v = c->self;
     for (int b = 0; b < v->nblocks; ++b) {
         DerivedArgs A{};
@@ -791,7 +814,12 @@ void wm_batch_destroy(wm_batch* b) { delete b; }
 
 int wm_batch_step(wm_batch* b, double* const* q_in, double* const* q_out, const double* const* dt_in,
                   double* const* dt_next, const double* times, void* stream) {
-    if (!b || !q_in || !q_out || !dt_in || !dt_next || !times) return fail(WM_E_INVALID, "null argument");
+    if (!b || !times) return fail(WM_E_INVALID, "null argument");
+    const View& v = b->view;
+    if (int r = check_ptrs((const void* const*)q_in, v.nblocks, "q_in")) return r;
+    if (int r = check_ptrs((const void* const*)q_out, v.nblocks, "q_out")) return r;
+    if (int r = check_ptrs((const void* const*)dt_in, v.ncases, "dt_in")) return r;
+    if (int r = check_ptrs((const void* const*)dt_next, v.ncases, "dt_next")) return r;
     return run_step(&b->view, &b->prof, q_in, q_out, b->w0.data(), b->w1.data(), dt_in, dt_next, times, true,
                     (cudaStream_t)stream);
 }
