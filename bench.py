@@ -151,7 +151,7 @@ def run_ours(args, rank, world, local_rank):
     def max_over_ranks(x):
         return reduce_max(x, dist, dev)
 
-    mesh, gas, kw, prim = channel_case(2, n=N_CFG2)
+    mesh, gas, kw, prim = channel_case(2, n=N_CFG2, device=True)
     cells = int(np.prod(mesh.blocks[0].n))
     Q0h = [np.ascontiguousarray(gas.prim_to_cons(np.asarray(prim(g.xc), float))) for g in mesh.geoms]
     K, Wm = args.steps, args.warmup

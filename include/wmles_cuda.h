@@ -23,6 +23,7 @@
  *   wm_wall_stats    Solver.wall_stats          wmles/solver.py:163-179
  *   wm_plane_stats   PlaneStats.accumulate      wmles/channel5200.py:121-152
  *   wm_derived_fields derived_fields            wmles/io_vtk.py:269-293
+ *   wm_block_geometry Mesh.finalize metrics     wmles/mesh.py:53-73,213-242 (one block)
  */
 #ifndef WMLES_CUDA_H
 #define WMLES_CUDA_H
@@ -72,7 +73,8 @@ typedef struct {
 typedef struct {
     int n[3];                 /* interior cells per direction */
     int ng;                   /* ghost layers (the reference's ng = 3) */
-    const double* metrics;    /* host, WM_NMET x Ni x Nj x Nk */
+    const double* metrics;    /* WM_NMET x Ni x Nj x Nk, host or device memory (a device
+                                 table, e.g. from wm_block_geometry, is copied on the device) */
 } wm_block;
 
 typedef struct {
@@ -203,6 +205,18 @@ int wm_plane_stats(wm_case* c, int block, const double* q, double* sum, void* st
  * Q-criterion.  q must have its first ghost layer filled (call wm_apply_bcs first, as the
  * reference does); it is not modified. */
 int wm_derived_fields(wm_case* c, const double* const* q, double* const* out, void* stream);
+
+/* Geometry of one block on the device (the metrics of Mesh.finalize, wmles/mesh.py:53-73,
+ * for one block whose ghost nodes are filled, wmles/mesh.py:213-242), with the host path's
+ * arithmetic: every output bit-identical to it except the filter width V^(1/3) of the
+ * packed table (device pow; within a few ulp).  N: cells per direction including ghosts
+ * (n + 2 ng).  Device float64 arrays, C order: X 3 x (N0+1) x (N1+1) x (N2+1) nodes;
+ * vol N0 x N1 x N2; xc 3 x N0 x N1 x N2; S[d], xf[d] 3 x (N0 + (d==0)) x (N1 + (d==1)) x
+ * (N2 + (d==2)) face area vectors and face centres along +d; met (NULL: not written)
+ * WM_NMET x N0 x N1 x N2, the packed table wm_block.metrics takes.  Asynchronous on the
+ * stream; allocates nothing. */
+int wm_block_geometry(const double* X, const int* N, double* vol, double* xc, double* const* S,
+                      double* const* xf, double* met, void* stream);
 
 /* Batched stepping of several resident cases (no reference counterpart: the reference
  * advances one case per Solver).  A wm_batch is a fixed set of cases that share the

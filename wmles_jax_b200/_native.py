@@ -75,6 +75,8 @@ SIGNATURES = {
     "wm_wall_stats": (C.c_int, [C.c_void_p, PP, PP, C.c_void_p]),
     "wm_plane_stats": (C.c_int, [C.c_void_p, C.c_int, c_double_p, c_double_p, C.c_void_p]),
     "wm_derived_fields": (C.c_int, [C.c_void_p, PP, PP, C.c_void_p]),
+    "wm_block_geometry": (C.c_int, [c_double_p, c_int_p, c_double_p, c_double_p, PP, PP, c_double_p,
+                                    C.c_void_p]),
     "wm_batch_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     "wm_batch_destroy": (None, [C.c_void_p]),
     "wm_batch_step": (C.c_int, [C.c_void_p, PP, PP, PP, PP, c_double_p, C.c_void_p]),

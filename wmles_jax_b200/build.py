@@ -2,8 +2,9 @@
 
     python -m wmles_jax_b200.build [--force] [--jobs N]
 
-Each .cu file in csrc/ is compiled separately (surface.cu with -fmad=false so that the
-ghost-cell maps round exactly like the reference's NumPy arithmetic; stage.cu with fast
+Each .cu file in csrc/ is compiled separately (surface.cu and geom.cu with -fmad=false so
+that the ghost-cell maps and the block geometry round exactly like the reference's NumPy
+arithmetic; stage.cu with fast
 single-precision division and square root for the mixed form), then linked into
 wmles_jax_b200/libwmles_cuda.so against the shared CUDA runtime.
 """
@@ -25,7 +26,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relax
 # denormals flushed.  These options act on FP32 operations only: the FP64 stage kernels are
 # unchanged, and the mixed form's FP32 fluxes, gradients and SGS are judged against FP64
 # at a tolerance far above the last-place error of these instructions.
-PER_FILE = {"surface.cu": ["-fmad=false"],
+PER_FILE = {"surface.cu": ["-fmad=false"], "geom.cu": ["-fmad=false"],
             "stage.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]}
 
 

@@ -22,6 +22,7 @@
 #include "aux.cuh"
 #include "stats.cuh"
 #include "derived.cuh"
+#include "geom.cuh"
 
 using namespace wm;
 
@@ -600,15 +601,22 @@ int wm_case_create(const wm_case_desc* d, wm_case** out) {
         if (B.ncell * WM_NMET >= (1LL << 31))
             return bail(fail(WM_E_UNSUPPORTED, "block %d: %lld cells exceed the 32-bit metric index range "
                              "(split the block)", b, B.ncell));
+        // the metric table may sit in host or device memory (wm_block_geometry's output);
+        // the mixed form's FP32 copy is rounded on the device from the case's FP64 copy
+        const size_t nmet = (size_t)WM_NMET * B.ncell;
+        cudaPointerAttributes pa{};
+        CKB(cudaPointerGetAttributes(&pa, src.metrics));
+        const bool on_device = pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged;
         double* met = nullptr;
-        if ((r = c->mem.upload(&met, src.metrics, (size_t)WM_NMET * B.ncell))) return bail(r);
+        if ((r = c->mem.alloc(&met, nmet))) return bail(r);
+        CKB(cudaMemcpy(met, src.metrics, sizeof(double) * nmet,
+                       on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice));
         B.met = met;
         B.met32 = nullptr;
         if (d->precision == WM_PREC_MIXED) {
-            std::vector<float> m32((size_t)WM_NMET * B.ncell);
-            for (size_t i = 0; i < m32.size(); ++i) m32[i] = (float)src.metrics[i];
             float* p32 = nullptr;
-            if ((r = c->mem.upload(&p32, m32.data(), m32.size()))) return bail(r);
+            if ((r = c->mem.alloc(&p32, nmet))) return bail(r);
+            CKB(launch_to_f32(met, p32, (long long)nmet, 0));
             B.met32 = p32;
         }
         for (int s = 0; s < 2; ++s) {
@@ -792,6 +800,25 @@ int wm_derived_fields(wm_case* c, const double* const* q, double* const* out, vo
         const BlockDev& B = v->hb[b];
         CK(launch_derived(A, (long long)B.n[0] * B.n[1] * B.n[2], (cudaStream_t)stream));
     }
+    return WM_OK;
+}
+
+int wm_block_geometry(const double* X, const int* N, double* vol, double* xc, double* const* S,
+                      double* const* xf, double* met, void* stream) {
+    if (!X || !N || !vol || !xc || !S || !xf) return fail(WM_E_INVALID, "null argument");
+    GeomArgs A{};
+    A.X = X;
+    for (int d = 0; d < 3; ++d) {
+        if (N[d] < 1) return fail(WM_E_INVALID, "N[%d] = %d: every direction needs a cell", d, N[d]);
+        if (!S[d] || !xf[d]) return fail(WM_E_INVALID, "null face array of direction %d", d);
+        A.N[d] = N[d];
+        A.S[d] = S[d];
+        A.xf[d] = xf[d];
+    }
+    A.vol = vol;
+    A.xc = xc;
+    A.met = met;
+    CK(launch_geometry(A, (cudaStream_t)stream));
     return WM_OK;
 }
 

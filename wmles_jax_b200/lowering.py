@@ -41,7 +41,11 @@ def share_metrics(mesh):
 
 
 def block_metrics(blk, geom):
-    """(NMET, Ni, Nj, Nk) float64 metric array of one block."""
+    """(NMET, Ni, Nj, Nk) float64 metric array of one block: the device table kept by
+    Mesh.finalize(device=True) when the block has one for this geometry, else a host array."""
+    dev = getattr(blk, "metrics_dev", None)
+    if dev is not None and blk.geom is geom:
+        return dev
     ent = _SHARED.get(id(geom))
     if ent is not None and ent[0] is geom:
         if ent[1] is None:

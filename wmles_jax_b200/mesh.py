@@ -2,8 +2,9 @@
 
 API of the reference (wmles/mesh.py): ``Block(name, nodes, ng=3)``, ``Block.set_bc``,
 ``Mesh(blocks)``, ``Mesh.connect(A, faceA, B, faceB, shift)``, ``Mesh.finalize()``, and a
-``Geom(vol, xc, S, xf)`` per block.  Set-up runs once on the host; its result feeds the
-device metric arrays built by ``wmles_jax_b200.lowering``.
+``Geom(vol, xc, S, xf)`` per block.  Set-up runs once, on the host or, with
+``finalize(device=True)``, with the metrics computed on the GPU (same bits); its result
+feeds the device metric arrays built by ``wmles_jax_b200.lowering``.
 
 Every block-to-block copy (ghost nodes here, ghost cells in the ghost-gather program)
 is expressed as an *index map*: the flat source indices that land in each destination
@@ -120,6 +121,7 @@ class Block:
         self.faces = {}
         self.X = None
         self.geom = None
+        self.metrics_dev = None
 
     def set_bc(self, face, bc):
         self.faces[FACE_NAMES[face]] = bc
@@ -233,9 +235,14 @@ class Mesh:
             mapping, flip = _match_orientation(X, fx, Y, fy, sh)
             X.faces[fx] = Interface(self.index(Y), fy, mapping, flip, sh)
 
-    def finalize(self, node_passes=3):
+    def finalize(self, node_passes=3, device=False):
         """Ghost nodes (node_passes sweeps of exchange / reflection) and metrics;
-        wmles/mesh.py:213-242."""
+        wmles/mesh.py:213-242.
+
+        device=True computes the metrics on the GPU (``device_geometry.block_geometry``):
+        the ``Geom`` arrays are the same bits, and each block keeps its packed metric table
+        on the device (``Block.metrics_dev``, 216 B per cell including ghosts) for the
+        solvers built on this mesh; ``release_device_metrics`` frees it."""
         ng = self.ng
         for b in self.blocks:
             for f in FACE_NAMES.values():
@@ -244,26 +251,41 @@ class Mesh:
             X = np.zeros((3,) + tuple(n + 1 + 2 * ng for n in b.n))
             X[(slice(None),) + tuple(slice(ng, ng + n + 1) for n in b.n)] = b.x_int
             b.X = X
+        maps = {}      # the index maps are the same on every pass
         for _ in range(node_passes):
             for a in range(3):
-                for b in self.blocks:
+                for ib, b in enumerate(self.blocks):
                     for s in (0, 1):
                         f = b.faces[(a, s)]
                         if isinstance(f, Interface):
                             src = self.blocks[f.nb]
-                            dst_flat, src_flat = interface_index_map(
-                                b.X.shape[1:], src.X.shape[1:], ng, b.n[a], src.n[f.src_face[0]],
-                                (a, s), f, "node")
+                            key = (ib, a, s)
+                            if key not in maps:
+                                maps[key] = interface_index_map(
+                                    b.X.shape[1:], src.X.shape[1:], ng, b.n[a], src.n[f.src_face[0]],
+                                    (a, s), f, "node")
+                            dst_flat, src_flat = maps[key]
                             vals = src.X.reshape(3, -1)[:, src_flat] + f.shift.reshape(3, 1)
                             b.X.reshape(3, -1)[:, dst_flat] = vals
                         else:
                             _reflect_nodes(b.X, b, a, s)
         geoms = []
         for b in self.blocks:
-            vol, xc, S, xf = compute_geometry(b.X)
+            if device:
+                from .device_geometry import block_geometry
+                (vol, xc, S, xf), b.metrics_dev = block_geometry(b.X)
+            else:
+                vol, xc, S, xf = compute_geometry(b.X)
+                b.metrics_dev = None
             if vol.min() <= 0:
                 raise ValueError(f"block {b.name}: non-positive cell volume (left-handed or folded grid)")
             b.geom = Geom(vol, xc, S, xf)
             geoms.append(b.geom)
         self.geoms = tuple(geoms)
         return self
+
+    def release_device_metrics(self):
+        """Free the packed metric tables kept on the device by finalize(device=True)
+        (solvers already built keep their own copies)."""
+        for b in self.blocks:
+            b.metrics_dev = None

@@ -27,12 +27,12 @@ from .workloads import channel_case, naca_case, ramp_case
 
 def build(config, n=None, scale=1):
     if config == 2:
-        return channel_case(2, n=tuple(n) if n else (256, 128, 128))
+        return channel_case(2, n=tuple(n) if n else (256, 128, 128), device=True)
     if config == 3:
-        mesh, gas, kw, prim, _ = ramp_case(tuple(n) if n else (384, 96, 64))
+        mesh, gas, kw, prim, _ = ramp_case(tuple(n) if n else (384, 96, 64), device=True)
         return mesh, gas, kw, prim
     if config == 4:
-        return naca_case(scale=scale)
+        return naca_case(scale=scale, device=True)
     raise ValueError(f"unknown config {config}")
 
 

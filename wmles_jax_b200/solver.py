@@ -132,7 +132,14 @@ class Solver:
         for ib, (b, geo) in enumerate(zip(self.blocks, self.geoms)):
             blocks[ib].n = (C.c_int * 3)(*b.n)
             blocks[ib].ng = b.ng
-            blocks[ib].metrics = N.as_double_p(self._arr(block_metrics(b, geo), np.float64))
+            met = block_metrics(b, geo)
+            if isinstance(met, torch.Tensor):                 # device table (finalize(device=True))
+                if met.device != self.device or met.dtype != torch.float64 or not met.is_contiguous():
+                    raise ValueError(f"block {b.name}: device metric table on {met.device}, {met.dtype}")
+                self._keep.append(met)
+                blocks[ib].metrics = C.cast(C.c_void_p(met.data_ptr()), N.c_double_p)
+            else:
+                blocks[ib].metrics = N.as_double_p(self._arr(met, np.float64))
         self._keep.append(blocks)
         d.nblocks, d.blocks = nb, blocks
         # wall-modelled faces

@@ -27,7 +27,7 @@ def channel_gas(Ma_b=0.3, Re_b=20000.0, gamma=1.4):
     return Gas(gamma=gamma, R=1.0 / (gamma * Ma_b ** 2), mu_ref=1.0 / Re_b, T_ref=1.0, S_suth=110.4 / 300.0)
 
 
-def channel_mesh(n, blocks=1, beta=2.0, n_match=3, T_wall=1.0, Lx=2 * np.pi, Lz=np.pi):
+def channel_mesh(n, blocks=1, beta=2.0, n_match=3, T_wall=1.0, Lx=2 * np.pi, Lz=np.pi, device=False):
     nx, ny, nz = n
     if nx % blocks:
         raise ValueError("nx must divide into the blocks")
@@ -47,7 +47,7 @@ def channel_mesh(n, blocks=1, beta=2.0, n_match=3, T_wall=1.0, Lx=2 * np.pi, Lz=
         mesh.connect(blk, "kmin", blk, "kmax", shift=(0, 0, -Lz))
         blk.set_bc("jmin", WallModel(wm, T_wall=T_wall, n_match=n_match))
         blk.set_bc("jmax", WallModel(wm, T_wall=T_wall, n_match=n_match))
-    return mesh.finalize()
+    return mesh.finalize(device=device)
 
 
 def spalding_uplus(yp, kappa=0.41, B=5.2, iters=60):
@@ -93,11 +93,12 @@ def loglaw_prim(gas, mesh, noise=0.1, seed=0):
     return prim
 
 
-def channel_case(config=2, n=None, blocks=None):
-    """(mesh, gas, solver kwargs, prim_fn) of channel config 1 or 2 (optionally resized)."""
+def channel_case(config=2, n=None, blocks=None, device=False):
+    """(mesh, gas, solver kwargs, prim_fn) of channel config 1 or 2 (optionally resized);
+    device=True computes the mesh metrics on the GPU (Mesh.finalize)."""
     gas = channel_gas()
     if config == 1:
-        mesh = channel_mesh(n or (32, 32, 16), blocks=blocks or 2, beta=2.0)
+        mesh = channel_mesh(n or (32, 32, 16), blocks=blocks or 2, beta=2.0, device=device)
         from .sgs import make_sgs  # noqa: F401  (names resolved by the solver)
         kw = dict(scheme=KEP(2), sgs="smagorinsky", sgs_kwargs=dict(Cs=0.1), cfl=0.5,
                   constraints=[ConstantMassFlux(0, 1.0)])
@@ -109,7 +110,7 @@ def channel_case(config=2, n=None, blocks=None):
             one = np.ones_like(y)
             return np.stack([one, 1.5 * y * (2.0 - y) + pert[0], pert[1], pert[2], gas.R * one])
         return mesh, gas, kw, prim
-    mesh = channel_mesh(n or (256, 128, 128), blocks=blocks or 1, beta=2.5)
+    mesh = channel_mesh(n or (256, 128, 128), blocks=blocks or 1, beta=2.5, device=device)
     kw = dict(scheme=KEP(4), sgs="wale", sgs_kwargs=dict(Cw=0.5), cfl=0.5,
               constraints=[ConstantMassFlux(0, 1.0)])
     return mesh, gas, kw, loglaw_prim(gas, mesh)
@@ -162,7 +163,7 @@ def ramp_nodes(n, x_range=(-0.76, 4.0), ratio=1.08, L=1.0):
     return np.stack((X, Y, Z)) * L
 
 
-def ramp_case(n=(384, 96, 64), n_modes=64, seed=0, sponge_start_l=3.0, x_range=(-0.76, 4.0)):
+def ramp_case(n=(384, 96, 64), n_modes=64, seed=0, sponge_start_l=3.0, x_range=(-0.76, 4.0), device=False):
     """(mesh, gas, solver kwargs, prim_fn, props) of the smooth-ramp configuration (config 3
     at the default size): quintic ramp wall with the equilibrium wall model (adiabatic,
     sampled at the first cell), slip top at y = 0.74 L, periodic span 0.288 L, geometric
@@ -185,7 +186,7 @@ def ramp_case(n=(384, 96, 64), n_modes=64, seed=0, sponge_start_l=3.0, x_range=(
     blk.set_bc("imax", CharacteristicFarfield(prim_inf))
     blk.set_bc("jmin", WallModel(EquilibriumWallModel(), T_wall=None, n_match=1))
     blk.set_bc("jmax", SlipWall())
-    mesh.finalize()
+    mesh.finalize(device=device)
     sponge = SmoothRampSponge(props, sponge_start_l, x_range[1], 1.0)
     kw = dict(scheme=Hybrid(KEP(4)), sgs="vreman", cfl=0.5, sources=(sponge,))
     rng = np.random.default_rng(seed)
@@ -282,7 +283,8 @@ def _classes(api):
                                  CharacteristicFarfield=CharacteristicFarfield)
 
 
-def naca_case(scale=1, alpha_deg=4.0, Ma=0.15, Re_c=1e6, noise=0.01, seed=0, n_match=3, api=None):
+def naca_case(scale=1, alpha_deg=4.0, Ma=0.15, Re_c=1e6, noise=0.01, seed=0, n_match=3, api=None,
+              device=False):
     """(mesh, gas, solver kwargs, prim_fn) of the NACA 0012 C-grid (config 4 at scale 1):
     nondimensional gas (rho = T = 1 gives |U| = 1 at Ma, Re on the chord), angle of attack
     `alpha_deg`, adiabatic equilibrium wall model on the section, characteristic far field
@@ -310,7 +312,7 @@ def naca_case(scale=1, alpha_deg=4.0, Ma=0.15, Re_c=1e6, noise=0.01, seed=0, n_m
     aft.set_bc("imin", WallModel(wm, T_wall=None, n_match=m))
     for b, f in ((sec, "jmax"), (wl, "jmin"), (wl, "imax"), (wu, "jmax"), (wu, "imax"), (aft, "imax")):
         b.set_bc(f, CharacteristicFarfield(prim_inf))
-    mesh.finalize()
+    mesh.finalize(device=True) if device else mesh.finalize()
     kw = dict(scheme=Hybrid(KEP(4)), sgs="vreman", cfl=0.5)
     rng = np.random.default_rng(seed)
 
@@ -340,10 +342,11 @@ def re_bulk_from_re_tau(re_tau):
 
 @functools.lru_cache(maxsize=16)
 def serving_mesh(grid):
-    """Finalized channel mesh of one serving grid, built once and shared by every request on
-    that grid (the geometry does not depend on Re_tau or Ma_b); its packed metrics are kept."""
+    """Finalized channel mesh of one serving grid, built once (metrics on the GPU) and shared
+    by every request on that grid (the geometry does not depend on Re_tau or Ma_b); its packed
+    metrics stay on the device."""
     from .lowering import share_metrics
-    mesh = channel_mesh(grid, blocks=1, beta=2.5)
+    mesh = channel_mesh(grid, blocks=1, beta=2.5, device=True)
     share_metrics(mesh)
     return mesh
 
