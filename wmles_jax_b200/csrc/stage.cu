@@ -37,9 +37,22 @@ constexpr int stage_min_ctas(size_t rsize, int nt) {
     return rsize == 4 ? (nt <= 128 ? 3 : (nt <= 256 ? 2 : 1)) : (nt <= 128 ? 2 : 1);
 }
 
+// warps per CTA beyond the tile's columns: they take a share of every flat loop (primitive
+// conversion, gradient records, j/k faces), so a plane's rounds of work are fuller (the 340
+// gradient records of an 8 x 32 tile fit one round of 352 threads) and more warps hide the
+// FP64 latency; the column-bound work (i-face flux, RK epilogue) stays with the first
+// TJ x TK threads.  FP64 256-column tiles only: the single resident CTA then runs with 168
+// registers per thread (no spills for KEP, ~200 B for MUSCL / Hybrid, still faster:
+// config 2 stage time -9 %, configs 3 and 4 -7 % and -5.5 %); the float form, two CTAs per
+// SM, gains nothing measurable.
+constexpr int stage_extra_warps(size_t rsize, int scheme, int nt) {
+    return (rsize == 8 && nt == 256) ? 3 : 0;
+}
+
 template <typename R, int SCHEME, int TJ, int TK>
 struct StageLayout {
-    static constexpr int NT = TJ * TK;
+    static constexpr int NT = TJ * TK;                                         // tile columns
+    static constexpr int NTH = NT + 32 * stage_extra_warps(sizeof(R), SCHEME, NT);   // threads
     static constexpr int PJ = TJ + 4, PK = TK + 4, PN = PJ * PK;   // primitives: 2-cell halo
     static constexpr int GJ = TJ + 2, GK = TK + 2, GN = GJ * GK;   // gradients: 1-cell halo
     static constexpr int NGS = (SCHEME == WM_SCHEME_HYBRID) ? 15 : 14;
@@ -54,7 +67,8 @@ struct StageLayout {
     // resident CTAs per SM the register budget is sized for: the FP64 form of the 256-thread
     // tiles needs ~250 registers and 170+ KB of shared memory (one CTA); the float form
     // fits two 256-thread CTAs (<= 128 registers, ~96 KB each) or three 128-thread CTAs
-    static constexpr int MIN_CTAS = stage_min_ctas(sizeof(R), NT);
+    static constexpr int MIN_CTAS = stage_min_ctas(sizeof(R), NTH);
+    static_assert(2 * (NTH / 32) <= 32, "the reduction scratch holds two sums per warp");
 };
 
 // gradient record: g[0..11] = d(u,v,w,T)/d(x,y,z), 12 = mu_eff, 13 = k_eff, 14 = theta
@@ -136,10 +150,10 @@ __device__ __forceinline__ void face_flux(const StageOpts& o, const Phys<R>& P, 
 }
 
 template <typename R, int SCHEME, int TJ, int TK>
-__global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
+__global__ void __launch_bounds__(StageLayout<R, SCHEME, TJ, TK>::NTH, StageLayout<R, SCHEME, TJ, TK>::MIN_CTAS)
     stage_kernel(const __grid_constant__ StageArgs A, const StageOpts o) {
     using LY = StageLayout<R, SCHEME, TJ, TK>;
-    constexpr int NT = LY::NT, PK = LY::PK, PN = LY::PN, GK = LY::GK, GN = LY::GN, NGS = LY::NGS;
+    constexpr int NT = LY::NT, NTH = LY::NTH, PK = LY::PK, PN = LY::PN, GK = LY::GK, GN = LY::GN, NGS = LY::NGS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* qs = reinterpret_cast<double*>(smem_raw + LY::qs_off);
     R* pr = reinterpret_cast<R*>(smem_raw + LY::pr_off);
@@ -162,12 +176,13 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
     const int tid = threadIdx.x, tj = tid / TK, tk = tid % TK;
     const int jhi = ng + B.n[1], khi = ng + B.n[2], ihi = ng + B.n[0];
     const int j = t.j0 + tj, k = t.k0 + tk;
-    const bool active = (j < jhi) && (k < khi);
+    const bool column = tid < NT;                  // this thread owns a tile column
+    const bool active = column && (j < jhi) && (k < khi);
     const int sgs_model = o.sgs;
 
     // ---- conservative values of plane ip on the tile + 2-cell halo -> staging buffer (async)
     auto stage_plane = [&](int ip) {
-        for (int c = tid; c < PN; c += NT) {
+        for (int c = tid; c < PN; c += NTH) {
             const int jj = c / PK, kk = c - jj * PK;
             const int gj = min(max(t.j0 - 2 + jj, 0), Nj - 1);
             const int gk = min(max(t.k0 - 2 + kk, 0), Nk - 1);
@@ -179,7 +194,7 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
     // ---- staged values -> primitive records in ring slot
     auto convert_plane = [&](int slot) {
         R* dst = pr + slot * PR_N * PN;
-        for (int c = tid; c < PN; c += NT) {
+        for (int c = tid; c < PN; c += NTH) {
             double q[5];
 #pragma unroll
             for (int v = 0; v < 5; ++v) q[v] = qs[v * PN + c];
@@ -195,7 +210,7 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
         const R* Pm = pr + ((ip - 1) & 3) * PR_N * PN;
         const R* P0 = pr + (ip & 3) * PR_N * PN;
         const R* Pp = pr + ((ip + 1) & 3) * PR_N * PN;
-        for (int c = tid; c < GN; c += NT) {
+        for (int c = tid; c < GN; c += NTH) {
             const int jj = c / GK, kk = c - jj * GK;
             const int pc = (jj + 1) * PK + (kk + 1);
             const int gj = min(t.j0 - 1 + jj, Nj - 2), gk = min(t.k0 - 1 + kk, Nk - 2);
@@ -331,7 +346,7 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
         // components read by the stage kernel: S (0..8), delta, 1/V, e/idist (13..26) of plane
         // ip+1 (23), then S_i (0..2) of plane ip+2 (3)
         constexpr int NPF = 26;
-        for (int it = tid; it < NPF * ROWS * LINES; it += NT) {
+        for (int it = tid; it < NPF * ROWS * LINES; it += NTH) {
             const int comp = it / (ROWS * LINES), rem = it - comp * (ROWS * LINES);
             const int row = rem / LINES, line = rem - row * LINES;
             const int pl = comp < 23 ? ip + 1 : ip + 2;
@@ -344,7 +359,7 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
         }
         if (A.stage >= 2 && ip < ihi) {
             constexpr int QL = (TK * 8 + 127) / 128 + 1;
-            for (int it = tid; it < 5 * TJ * QL; it += NT) {
+            for (int it = tid; it < 5 * TJ * QL; it += NTH) {
                 const int v = it / (TJ * QL), rem = it - v * (TJ * QL);
                 const int row = rem / QL, line = rem - row * QL;
                 const int gj = min(t.j0 + row, Nj - 1);
@@ -356,6 +371,7 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
     };
 
     auto save_gs = [&]() {
+        if (!column) return;
         const int gc = (tj + 1) * GK + (tk + 1);
 #pragma unroll
         for (int v = 0; v < NGS; ++v) gsp[v] = gs[v * GN + gc];
@@ -363,6 +379,7 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
 
     R dFj[5], dFk[5], Flo[5];
     auto jk_diff = [&]() {
+        if (!column) return;
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
             dFj[v] = fj[v * LY::FJN + (tj + 1) * TK + tk] - fj[v * LY::FJN + tj * TK + tk];
@@ -445,7 +462,7 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
     grad_plane(i0);
     __syncthreads();
     if (active) iface_flux(i0, Flo);
-    for (int f = tid; f < LY::FJN + LY::FKN; f += NT) jk_face(i0, f);
+    for (int f = tid; f < LY::FJN + LY::FKN; f += NTH) jk_face(i0, f);
     cp_async_wait_all();
     __syncthreads();
     jk_diff();
@@ -471,16 +488,16 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) cmf_acc += __shfl_down_sync(0xffffffffu, cmf_acc, off);
             // warp sums of this plane; two buffers by plane parity (read after the barrier below)
-            if ((tid & 31) == 0) red[(ip & 1) * (NT / 32) + (tid >> 5)] = cmf_acc;
+            if ((tid & 31) == 0) red[(ip & 1) * (NTH / 32) + (tid >> 5)] = cmf_acc;
             cmf_acc = 0.0;
         }
         if (ip < i1)
-            for (int f = tid; f < LY::FJN + LY::FKN; f += NT) jk_face(ip, f);
+            for (int f = tid; f < LY::FJN + LY::FKN; f += NTH) jk_face(ip, f);
         cp_async_wait_all();
         __syncthreads();
         if (cmf_on && tid == 0) {
             double sp = 0.0;
-            for (int w = 0; w < NT / 32; ++w) sp += red[(ip & 1) * (NT / 32) + w];
+            for (int w = 0; w < NTH / 32; ++w) sp += red[(ip & 1) * (NTH / 32) + w];
             cmf_col[ip - 1 - ng] = sp;
         }
         if (ip < i1) {
@@ -507,7 +524,7 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
                 if (Cc.cmf_dir < 0) continue;
                 const int s0 = A.case_slot_start[c], s1 = A.case_slot_start[c + 1];
                 double s = 0.0;
-                for (int i = s0 + tid; i < s1; i += NT) s += part[i];
+                for (int i = s0 + tid; i < s1; i += NTH) s += part[i];
 #pragma unroll
                 for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
                 __syncthreads();
@@ -515,7 +532,7 @@ __global__ void __launch_bounds__(TJ* TK, stage_min_ctas(sizeof(R), TJ* TK))
                 __syncthreads();
                 if (tid == 0) {
                     double tot = 0.0;
-                    for (int w = 0; w < NT / 32; ++w) tot += red[w];
+                    for (int w = 0; w < NTH / 32; ++w) tot += red[w];
                     A.cmf_delta[c] = Cc.cmf_target - tot / Cc.cmf_volume;
                 }
             }
@@ -542,7 +559,7 @@ static cudaError_t launch_one(const StageArgs& A, const StageOpts& o, cudaStream
     using LY = StageLayout<R, SCHEME, TJ, TK>;
     cudaError_t e = configure_one<R, SCHEME, TJ, TK>();
     if (e != cudaSuccess) return e;
-    stage_kernel<R, SCHEME, TJ, TK><<<A.ntiles, LY::NT, LY::bytes, s>>>(A, o);
+    stage_kernel<R, SCHEME, TJ, TK><<<A.ntiles, LY::NTH, LY::bytes, s>>>(A, o);
     return cudaGetLastError();
 }
 
@@ -551,7 +568,7 @@ static int occupancy_one() {
     using LY = StageLayout<R, SCHEME, TJ, TK>;
     if (configure_one<R, SCHEME, TJ, TK>() != cudaSuccess) return 1;
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage_kernel<R, SCHEME, TJ, TK>, LY::NT, LY::bytes) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage_kernel<R, SCHEME, TJ, TK>, LY::NTH, LY::bytes) !=
         cudaSuccess)
         return 1;
     return n;
