@@ -177,6 +177,9 @@ __global__ void __launch_bounds__(StageLayout<R, SCHEME, TJ, TK>::NTH, StageLayo
     const int jhi = ng + B.n[1], khi = ng + B.n[2], ihi = ng + B.n[0];
     const int j = t.j0 + tj, k = t.k0 + tk;
     const bool column = tid < NT;                  // this thread owns a tile column
+    // j/k-face loop index: the extra warps (no i-face flux of their own) come first, so the
+    // face work of a plane is spread more evenly over the threads
+    const int rtid = column ? tid + (NTH - NT) : tid - NT;
     const bool active = column && (j < jhi) && (k < khi);
     const int sgs_model = o.sgs;
 
@@ -462,7 +465,7 @@ __global__ void __launch_bounds__(StageLayout<R, SCHEME, TJ, TK>::NTH, StageLayo
     grad_plane(i0);
     __syncthreads();
     if (active) iface_flux(i0, Flo);
-    for (int f = tid; f < LY::FJN + LY::FKN; f += NTH) jk_face(i0, f);
+    for (int f = rtid; f < LY::FJN + LY::FKN; f += NTH) jk_face(i0, f);
     cp_async_wait_all();
     __syncthreads();
     jk_diff();
@@ -492,7 +495,7 @@ __global__ void __launch_bounds__(StageLayout<R, SCHEME, TJ, TK>::NTH, StageLayo
             cmf_acc = 0.0;
         }
         if (ip < i1)
-            for (int f = tid; f < LY::FJN + LY::FKN; f += NTH) jk_face(ip, f);
+            for (int f = rtid; f < LY::FJN + LY::FKN; f += NTH) jk_face(ip, f);
         cp_async_wait_all();
         __syncthreads();
         if (cmf_on && tid == 0) {
