@@ -38,21 +38,26 @@ constexpr int stage_min_ctas(size_t rsize, int nt) {
 }
 
 // warps per CTA beyond the tile's columns: they take a share of every flat loop (primitive
-// conversion, gradient records, j/k faces), so a plane's rounds of work are fuller (the 340
-// gradient records of an 8 x 32 tile fit one round of 352 threads) and more warps hide the
-// FP64 latency; the column-bound work (i-face flux, RK epilogue) stays with the first
-// TJ x TK threads.  FP64 256-column tiles only: the single resident CTA then runs with 168
-// registers per thread (no spills for KEP, ~200 B for MUSCL / Hybrid, still faster:
-// config 2 stage time -9 %, configs 3 and 4 -7 % and -5.5 %); the float form, two CTAs per
-// SM, gains nothing measurable.
-constexpr int stage_extra_warps(size_t rsize, int scheme, int nt) {
-    return (rsize == 8 && nt == 256) ? 3 : 0;
+// conversion, gradient records, j/k faces), so a plane's rounds of work are fuller and more
+// warps hide the FP64 latency; the column-bound work (i-face flux, RK epilogue) stays with
+// the first TJ x TK threads.  FP64 256-column tiles only, where one CTA per SM is resident.
+// The launch bound of the larger CTA holds the kernel at 168 (352 threads) or 128 registers
+// (448, 512 threads), with up to ~580 B of spills at 128, and it is still faster.  Measured
+// stage time per step, 8 x 32 tile (config 2 KEP / config 3 / config 4 Hybrid): 3.17 / 3.37 /
+// 3.72 ms at 256 threads (254 registers), 2.81 / 3.08 / 3.74 at 352, 2.65 / 2.81 / 3.20 at
+// 448, 2.67 / 2.78 / 3.03 at 512; 16 x 16 tile: KEP 2.93 at 448 (3.03 at 352), Hybrid
+// 3.12 / 2.61 at 352 (3.17 / 2.77 at 384, 3.52 / 2.85 at 512).  The float form (two CTAs per
+// SM, issue-bound rather than latency-bound) gains nothing measurable and keeps 256.
+constexpr int stage_extra_warps(size_t rsize, int scheme, int tj, int tk) {
+    if (rsize != 8 || tj * tk != 256) return 0;
+    if (scheme == WM_SCHEME_KEP) return 6;
+    return tj == 8 ? 8 : 3;
 }
 
 template <typename R, int SCHEME, int TJ, int TK>
 struct StageLayout {
     static constexpr int NT = TJ * TK;                                         // tile columns
-    static constexpr int NTH = NT + 32 * stage_extra_warps(sizeof(R), SCHEME, NT);   // threads
+    static constexpr int NTH = NT + 32 * stage_extra_warps(sizeof(R), SCHEME, TJ, TK);   // threads
     static constexpr int PJ = TJ + 4, PK = TK + 4, PN = PJ * PK;   // primitives: 2-cell halo
     static constexpr int GJ = TJ + 2, GK = TK + 2, GN = GJ * GK;   // gradients: 1-cell halo
     static constexpr int NGS = (SCHEME == WM_SCHEME_HYBRID) ? 15 : 14;
@@ -270,6 +275,8 @@ __global__ void __launch_bounds__(StageLayout<R, SCHEME, TJ, TK>::NTH, StageLayo
 
     // ---- i-face flux between planes ip-1 and ip for this thread's column
     R gsp[NGS];   // gradient record of plane ip-1 at this column
+#pragma unroll
+    for (int v = 0; v < NGS; ++v) gsp[v] = R(0);
     auto iface_flux = [&](int ip, R F[5]) {
         if (ip == ng && wall_flux(0, j, k, F)) return;
         if (ip == ihi && wall_flux(1, j, k, F)) return;
