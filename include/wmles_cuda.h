@@ -134,7 +134,9 @@ typedef struct {
     wm_ghost_program ghost_all;   /* every ghost cell (apply_bcs) */
     const wm_inflow* inflow;      /* NULL if no synthetic-turbulence inflow */
     wm_sponge sponge;
-    int tile;                 /* stage-kernel tile shape id, -1 = automatic */
+    int tile;                 /* stage-kernel tile shape id (0 = 8x32, 1 = 16x16, 2 = 4x32,
+                                 3 = 16x32, mixed form only); -1 = automatic: 0 for FP64,
+                                 3 for the mixed form */
     int chunk;                /* planes per CTA along i, 0 = automatic */
 } wm_case_desc;
 

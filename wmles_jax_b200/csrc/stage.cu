@@ -46,10 +46,15 @@ constexpr int stage_min_ctas(size_t rsize, int nt) {
 // stage time per step, 8 x 32 tile (config 2 KEP / config 3 / config 4 Hybrid): 3.17 / 3.37 /
 // 3.72 ms at 256 threads (254 registers), 2.81 / 3.08 / 3.74 at 352, 2.65 / 2.81 / 3.20 at
 // 448, 2.67 / 2.78 / 3.03 at 512; 16 x 16 tile: KEP 2.93 at 448 (3.03 at 352), Hybrid
-// 3.12 / 2.61 at 352 (3.17 / 2.77 at 384, 3.52 / 2.85 at 512).  The float form (two CTAs per
-// SM, issue-bound rather than latency-bound) gains nothing measurable and keeps 256.
+// 3.12 / 2.61 at 352 (3.17 / 2.77 at 384, 3.52 / 2.85 at 512).  The float form's two-CTA
+// tiles (issue-bound rather than latency-bound) gain nothing measurable and keep their
+// columns' threads; its one-CTA 16 x 32 tile runs 640 threads at 96 registers (mixed stage
+// time per step, configs 2 / 3 / 4: 1.52 / 1.23 / 1.14 ms, against 1.65 / 1.36 / 1.23 at
+// 512 threads and 1.58 / 1.31 / 1.21 for the best two-CTA tile).
+constexpr int STAGE_MAX_WARPS = 32;          // two reduction sums per warp in the scratch
 constexpr int stage_extra_warps(size_t rsize, int scheme, int tj, int tk) {
-    if (rsize != 8 || tj * tk != 256) return 0;
+    if (rsize == 4) return tj * tk == 512 ? 4 : 0;
+    if (tj * tk != 256) return 0;
     if (scheme == WM_SCHEME_KEP) return 6;
     return tj == 8 ? 8 : 3;
 }
@@ -68,12 +73,12 @@ struct StageLayout {
     static constexpr size_t fj_off = gs_off + sizeof(R) * NGS * GN;            // R [5][FJN]
     static constexpr size_t fk_off = fj_off + sizeof(R) * 5 * FJN;             // R [5][FKN]
     static constexpr size_t red_off = (fk_off + sizeof(R) * 5 * FKN + 15) / 16 * 16;
-    static constexpr size_t bytes = red_off + sizeof(double) * 32;
+    static constexpr size_t bytes = red_off + sizeof(double) * 2 * STAGE_MAX_WARPS;
     // resident CTAs per SM the register budget is sized for: the FP64 form of the 256-thread
     // tiles needs ~250 registers and 170+ KB of shared memory (one CTA); the float form
     // fits two 256-thread CTAs (<= 128 registers, ~96 KB each) or three 128-thread CTAs
     static constexpr int MIN_CTAS = stage_min_ctas(sizeof(R), NTH);
-    static_assert(2 * (NTH / 32) <= 32, "the reduction scratch holds two sums per warp");
+    static_assert(NTH / 32 <= STAGE_MAX_WARPS, "the reduction scratch holds two sums per warp");
 };
 
 // gradient record: g[0..11] = d(u,v,w,T)/d(x,y,z), 12 = mu_eff, 13 = k_eff, 14 = theta
