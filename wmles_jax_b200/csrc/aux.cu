@@ -33,31 +33,43 @@ template <> __device__ __forceinline__ const float* metrics_of<float>(const Bloc
 // min that propagates NaN like NumPy's np.min (a NaN time step must not be masked)
 __device__ __forceinline__ double nanmin(double a, double b) { return (a != a || a < b) ? a : b; }
 
-template <int NT>
-__device__ __forceinline__ double block_min(double v, double* red) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = nanmin(v, __shfl_down_sync(0xffffffffu, v, o));
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-    __syncthreads();
-    double m = DBL_MAX;
-    if (threadIdx.x == 0)
-        for (int w = 0; w < NT / 32; ++w) m = nanmin(m, red[w]);
-    return m;   // valid in thread 0
+// order-preserving 64-bit key of a double for an integer atomicMin: NaN gets the lowest key,
+// so a NaN time step wins the minimum as it does in NumPy's np.min
+__device__ __forceinline__ unsigned long long dt_key_of(double x) {
+    if (x != x) return 0ull;
+    const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double dt_value_of(unsigned long long k) {
+    if (k == 0ull) return __longlong_as_double(0x7ff8000000000000ll);
+    return __longlong_as_double((long long)((k >> 63) ? (k & 0x7fffffffffffffffull) : ~k));
 }
 
 // CFL time step (Solver._dt, wmles/solver.py:135-151), optionally after applying the
 // constant-mass-flux shift (ConstantMassFlux.__call__, wmles/solver.py:22-36) in place.
 // The view's interior cells are cut into chunks of DT_NT cells, one cell per thread, chunks
-// numbered block by block; one wave of resident CTAs walks the chunks (grid stride) and
-// writes each chunk's minimum, and the last CTA to finish reduces the minima per case.
-// M: the metric copy read (double; float for the mixed form); the arithmetic and the
-// reduction are FP64 either way.
+// numbered block by block (so case by case); one wave of resident CTAs walks the chunks
+// (grid stride).  Each thread keeps the minimum of its cells while the chunks stay in one
+// case; when the case changes and at the end, each warp folds its threads' minima and makes
+// one atomicMin on the case's key.  The last CTA to finish turns the keys into time steps
+// and resets them.  A minimum is exact in any order, so the result does not depend on the
+// grid, the chunking or the batch.  M: the metric copy read (double; float for the mixed
+// form); the arithmetic is FP64 either way.
 template <typename M>
 __global__ void __launch_bounds__(DT_NT) dt_kernel(const __grid_constant__ DtArgs D) {
-    __shared__ double red[2][DT_NT / 32];
     __shared__ bool last;
-    int parity = 0;
+    double run = DBL_MAX;          // this thread's minimum over its cells of case `cur`
+    int cur = -1;
+    auto flush = [&]() {
+        double m = run;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = nanmin(m, __shfl_down_sync(0xffffffffu, m, o));
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(D.dt_key + cur, dt_key_of(m));
+            __threadfence();
+        }
+        run = DBL_MAX;
+    };
 #pragma unroll 1
     for (int chunk = blockIdx.x; chunk < D.ncta; chunk += gridDim.x) {
         int b = 0;
@@ -69,13 +81,16 @@ __global__ void __launch_bounds__(DT_NT) dt_kernel(const __grid_constant__ DtArg
             }
         }
         const BlockDev& B = D.blocks[b];
+        if (D.want_dt && B.case_id != cur) {    // uniform over the CTA: one chunk at a time
+            if (cur >= 0) flush();
+            cur = B.case_id;
+        }
         const CaseDev& C = D.cases[B.case_id];
         const bool cmf = D.cmf_delta != nullptr && C.cmf_dir >= 0;
         const int ng = B.ng, nj = B.n[1], nk = B.n[2];
         const int Nk = B.N[2];
         const long long N = B.ncell, plane = B.plane;
         const long long ncells = (long long)B.n[0] * nj * nk;
-        double dtmin = DBL_MAX;
         const long long c = (long long)(chunk - D.cta_start[b]) * DT_NT + threadIdx.x;
         if (c < ncells) {
             double* q = D.q[b];
@@ -125,26 +140,13 @@ __global__ void __launch_bounds__(DT_NT) dt_kernel(const __grid_constant__ DtArg
                     lam = lam + fabs((u * sx + v * sy) + w * sz) + cs * Sm;
                     lamv = lamv + nu * (Sm * Sm) * ivol;
                 }
-                dtmin = C.cfl * vol / (lam + 4.0 * lamv);
+                run = nanmin(run, C.cfl * vol / (lam + 4.0 * lamv));
             }
-        }
-        if (D.want_dt) {
-            // chunk minimum: warp shuffles, then one barrier; the two shared buffers alternate
-            // so the next chunk's writes never meet this chunk's read by thread 0
-            double m = dtmin;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) m = nanmin(m, __shfl_down_sync(0xffffffffu, m, o));
-            if ((threadIdx.x & 31) == 0) red[parity][threadIdx.x >> 5] = m;
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                double mm = DBL_MAX;
-                for (int w = 0; w < DT_NT / 32; ++w) mm = nanmin(mm, red[parity][w]);
-                D.dt_part[chunk] = mm;
-            }
-            parity ^= 1;
         }
     }
     if (!D.want_dt) return;
+    if (cur >= 0) flush();
+    __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
         const unsigned prev = atomicAdd(D.counter, 1u);
@@ -152,16 +154,12 @@ __global__ void __launch_bounds__(DT_NT) dt_kernel(const __grid_constant__ DtArg
     }
     __syncthreads();
     if (last) {
-        // per case: the minimum over the chunks of that case's blocks
         __threadfence();
-        for (int c = 0; c < D.ncases; ++c) {
-            const int p0 = D.cta_start[D.case_block_start[c]];
-            const int p1 = D.cta_start[D.case_block_start[c + 1]];
-            double mm = DBL_MAX;
-            for (int i = p0 + threadIdx.x; i < p1; i += DT_NT) mm = nanmin(mm, ((volatile double*)D.dt_part)[i]);
-            mm = block_min<DT_NT>(mm, red[0]);
-            if (threadIdx.x == 0 && D.dt_out[c] != nullptr) D.dt_out[c][0] = mm;
-            __syncthreads();
+        for (int c = threadIdx.x; c < D.ncases; c += DT_NT) {
+            volatile unsigned long long* kp = D.dt_key + c;
+            const unsigned long long key = *kp;
+            if (D.dt_out[c] != nullptr) D.dt_out[c][0] = dt_value_of(key);
+            *kp = DT_KEY_EMPTY;
         }
         if (threadIdx.x == 0) *D.counter = 0u;
     }

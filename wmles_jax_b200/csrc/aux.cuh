@@ -36,10 +36,14 @@ struct DtArgs {
     const double* cmf_delta;       // per case: constant-mass-flux shift from stage 3 (null: none)
     int want_dt;                   // 0: constraint only
     int met32;                     // read the float metric copy (mixed form)
-    double* dt_part;               // per-CTA minima
+    unsigned long long* dt_key;    // per case: running minimum as an order-preserving key
+                                   // (DT_KEY_EMPTY between calls: reset by the last CTA)
     unsigned int* counter;         // last-CTA-done counter (reset by the last CTA)
     double* dt_out[MAX_CASES];     // per case: time step
 };
+
+// key of DBL_MAX, the value of an empty minimum (the reset value of DtArgs::dt_key)
+constexpr unsigned long long DT_KEY_EMPTY = 0xFFEFFFFFFFFFFFFFull;
 
 struct SpongeArgs {
     const BlockDev* blocks;

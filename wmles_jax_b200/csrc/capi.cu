@@ -184,7 +184,8 @@ struct View {
     Tile* d_tiles = nullptr;
     int* d_case_slot_start = nullptr;
     GhostSeg *d_seg_rhs = nullptr, *d_seg_all = nullptr;
-    double *cmf_part = nullptr, *cmf_delta = nullptr, *dt_part = nullptr;
+    double *cmf_part = nullptr, *cmf_delta = nullptr;
+    unsigned long long* dt_key = nullptr;   // CFL pass: per-case minimum keys
     unsigned* counters = nullptr;        // [0]: CFL reduction, [1]: constant-mass-flux reduction
     std::vector<int> cta_start;          // CFL pass: first CTA of each view block (+ total)
     int max_wall_faces = 0, sponge_rows = 0;
@@ -409,7 +410,10 @@ int build_view(View* v, wm_case* const* cases, int n) {
     if ((r = m.alloc(&v->cmf_part, (size_t)v->cmf_slot_start.back()))) return r;
     if ((r = m.alloc(&v->cmf_delta, (size_t)n))) return r;
     CK(cudaMemset(v->cmf_delta, 0, sizeof(double) * n));
-    if ((r = m.alloc(&v->dt_part, (size_t)v->cta_start.back()))) return r;
+    {
+        const std::vector<unsigned long long> empty((size_t)n, DT_KEY_EMPTY);
+        if ((r = m.upload(&v->dt_key, empty.data(), empty.size()))) return r;
+    }
     if ((r = m.alloc(&v->counters, 2))) return r;
     CK(cudaMemset(v->counters, 0, 2 * sizeof(unsigned)));
     return WM_OK;
@@ -497,7 +501,7 @@ int run_dt(View* v, Prof* pf, double* const* q, bool apply_cmf, bool want_dt, do
     D.cmf_delta = apply_cmf ? v->cmf_delta : nullptr;
     D.want_dt = want_dt ? 1 : 0;
     D.met32 = v->opts.precision == WM_PREC_MIXED ? 1 : 0;
-    D.dt_part = v->dt_part; D.counter = v->counters;
+    D.dt_key = v->dt_key; D.counter = v->counters;
     for (int ci = 0; ci < v->ncases; ++ci) D.dt_out[ci] = dt_out ? dt_out[ci] : nullptr;
     LaunchScope ls(pf, WM_KIND_DT, s);
     CK(launch_dt(D, s));
