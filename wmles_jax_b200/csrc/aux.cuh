@@ -47,6 +47,7 @@ constexpr unsigned long long DT_KEY_EMPTY = 0xFFEFFFFFFFFFFFFFull;
 
 struct SpongeArgs {
     const BlockDev* blocks;
+    const CaseDev* cases;
     int nblocks;
     const double* q[WM_MAX_BLOCKS];
     double* mean[WM_MAX_BLOCKS];   // 5 x Ni x Nj

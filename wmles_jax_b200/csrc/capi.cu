@@ -454,7 +454,7 @@ int run_stage(View* v, Prof* pf, int stage, double* const* q_in, const double* c
     for (int b = 0; b < v->nblocks; ++b) U.W.q[b] = q_in[b];
     std::vector<const double*> spm(v->nblocks, nullptr);
     if (v->any_sponge) {
-        U.S.blocks = v->d_blocks; U.S.nblocks = v->nblocks;
+        U.S.blocks = v->d_blocks; U.S.cases = v->d_cases; U.S.nblocks = v->nblocks;
         for (int ci = 0; ci < v->ncases; ++ci)
             for (size_t b = 0; b < v->members[ci]->hb.size(); ++b) {
                 const int vb = v->case_block_start[ci] + (int)b;
@@ -682,6 +682,8 @@ int wm_case_create(const wm_case_desc* d, wm_case** out) {
         for (int b = 0; b < d->nblocks; ++b) {
             const BlockDev& B = c->hb[b];
             if ((r = c->mem.alloc(&c->spmean[b], 5 * (size_t)B.N[0] * B.N[1]))) return bail(r);
+            // rows outside the sponge are never written (their mean is not needed): keep them 0
+            CKB(cudaMemset(c->spmean[b], 0, sizeof(double) * 5 * B.N[0] * B.N[1]));
         }
     }
 

@@ -255,6 +255,14 @@ __device__ __forceinline__ void sponge_row(const SpongeArgs& S, int b, int row, 
     const int i = row / nj + ng, j = row % nj + ng;
     const long long N = B.ncell;
     const long long base = i * B.plane + (long long)j * B.N[2];
+    // a row whose every cell lies before the sponge start needs no mean: the stage kernel's
+    // sponge term there is sigma * (q - mean) with sigma exactly 0 (the same expression as its
+    // ramp argument decides it), and the row's mean stays at its initial 0
+    const CaseDev& C = S.cases[B.case_id];
+    bool active = false;
+    for (int k = ng + lane; k < ng + nk; k += 32)
+        active |= (B.met[WM_MET_XCX * N + base + k] * C.sp_invL - C.sp_xs) * C.sp_inv_dx > 0.0;
+    if (!__any_sync(0xffffffffu, active)) return;
     const double* q = S.q[b];
     double acc[5] = {0, 0, 0, 0, 0}, vs = 0.0;
     for (int k = ng + lane; k < ng + nk; k += 32) {
