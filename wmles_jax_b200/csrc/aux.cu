@@ -188,24 +188,63 @@ cudaError_t launch_dt(const DtArgs& D, cudaStream_t s) {
 }
 
 // ------------------------------------------------------------------ synthetic inflow
-// SmoothRampInflow.fill_at_time / _unit_noise (wmles/smooth_ramp.py:150-197): one CTA per
-// (ghost layer, j) row, threads over k.
+// SmoothRampInflow.fill_at_time / _unit_noise (wmles/smooth_ramp.py:150-197), in two
+// launches: the mode sums (n_modes cosines per component and ghost cell) cut into IN_PARTS
+// contiguous mode ranges, one thread per (range, row, component, k), so that no thread
+// evaluates more than n_modes / IN_PARTS cosines; then one CTA per (ghost layer, j) row adds
+// the ranges in order, normalises the row and writes the ghost states.
 constexpr int IN_NT = 256;
 
-__device__ double interp_col(const double* tab, int n, double y, int col) {
-    // np.interp with end clamping on column 0 as abscissa
-    if (y <= tab[0]) return tab[col];
-    if (y >= tab[7 * (n - 1)]) return tab[7 * (n - 1) + col];
-    int lo = 0, hi = n - 1;
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (tab[7 * mid] <= y) lo = mid; else hi = mid;
-    }
-    const double x0 = tab[7 * lo], x1 = tab[7 * hi];
-    const double f0 = tab[7 * lo + col], f1 = tab[7 * hi + col];
-    const double slope = (f1 - f0) / (x1 - x0);
-    return slope * (y - x0) + f0;
+__global__ void __launch_bounds__(IN_NT) inflow_modes_kernel(const __grid_constant__ InflowArgs I, long long units) {
+    const long long u = (long long)blockIdx.x * IN_NT + threadIdx.x;
+    if (u >= units) return;
+    const BlockDev& B = *I.block;
+    const int ng = B.ng, Nj = B.N[1], Nk = B.N[2];
+    const long long rows = (long long)ng * Nj;
+    // u = ((part * rows + row) * 3 + c) * Nk + k, row = m * Nj + j
+    const int k = int(u % Nk);
+    const long long r1 = u / Nk;
+    const int c = int(r1 % 3);
+    const long long r2 = r1 / 3;
+    const int row = int(r2 % rows), pt = int(r2 / rows);
+    const int m = row / Nj, j = row - m * Nj, gi = ng - 1 - m;
+    const long long N = B.ncell;
+    const double time = I.time0 + I.time_dt * (I.dt ? *I.dt : 0.0);
+    const double X = I.U_inf * time / I.L;
+    const double* kx = I.modes + (c * 4 + 0) * I.n_modes;
+    const double* ky = I.modes + (c * 4 + 1) * I.n_modes;
+    const double* kz = I.modes + (c * 4 + 2) * I.n_modes;
+    const double* ph = I.modes + (c * 4 + 3) * I.n_modes;
+    const long long idx = ((long long)gi * Nj + j) * Nk + k;
+    const double y = B.met[WM_MET_XCY * N + idx] / I.L, z = B.met[WM_MET_XCZ * N + idx] / I.L;
+    const int per = (I.n_modes + IN_PARTS - 1) / IN_PARTS;
+    const int q1 = min(I.n_modes, (pt + 1) * per);
+    double acc = 0.0;
+    for (int q = pt * per; q < q1; ++q) acc += cos(((kx[q] * X + ky[q] * y) + kz[q] * z) + ph[q]);
+    I.raw[u] = acc;
 }
+
+// np.interp on the profile table (column 0 the abscissa, end values clamped): the bracket
+// of y is searched once per cell and shared by every column
+struct InterpAt {
+    int lo, hi;      // hi < 0: clamped to row lo
+    __device__ InterpAt(const double* tab, int n, double y) {
+        if (y <= tab[0]) { lo = 0; hi = -1; return; }
+        if (y >= tab[7 * (n - 1)]) { lo = n - 1; hi = -1; return; }
+        lo = 0; hi = n - 1;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (tab[7 * mid] <= y) lo = mid; else hi = mid;
+        }
+    }
+    __device__ double col(const double* tab, double y, int c) const {
+        if (hi < 0) return tab[7 * lo + c];
+        const double x0 = tab[7 * lo], x1 = tab[7 * hi];
+        const double f0 = tab[7 * lo + c], f1 = tab[7 * hi + c];
+        const double slope = (f1 - f0) / (x1 - x0);
+        return slope * (y - x0) + f0;
+    }
+};
 
 __global__ void __launch_bounds__(IN_NT) inflow_kernel(const __grid_constant__ InflowArgs I) {
     extern __shared__ double fsm[];            // 3 x Nk
@@ -214,21 +253,13 @@ __global__ void __launch_bounds__(IN_NT) inflow_kernel(const __grid_constant__ I
     const int ng = B.ng, Nj = B.N[1], Nk = B.N[2], nk = B.n[2];
     const int j = blockIdx.x, m = blockIdx.y, gi = ng - 1 - m;
     const long long N = B.ncell;
-    const double time = I.time0 + I.time_dt * (I.dt ? *I.dt : 0.0);
-    const double X = I.U_inf * time / I.L;
     double* f0 = fsm;
-    // raw mode sums of all three components at once: one (component, k) pair per thread
+    // raw mode sums of the row's three components: the partial sums added in range order
+    const long long rows = (long long)ng * Nj, row = (long long)m * Nj + j;
     for (int it = threadIdx.x; it < 3 * Nk; it += IN_NT) {
-        const int c = it / Nk, k = it - c * Nk;
-        const double* kx = I.modes + (c * 4 + 0) * I.n_modes;
-        const double* ky = I.modes + (c * 4 + 1) * I.n_modes;
-        const double* kz = I.modes + (c * 4 + 2) * I.n_modes;
-        const double* ph = I.modes + (c * 4 + 3) * I.n_modes;
-        const long long idx = ((long long)gi * Nj + j) * Nk + k;
-        const double y = B.met[WM_MET_XCY * N + idx] / I.L, z = B.met[WM_MET_XCZ * N + idx] / I.L;
-        double acc = 0.0;
-        for (int q = 0; q < I.n_modes; ++q) acc += cos(((kx[q] * X + ky[q] * y) + kz[q] * z) + ph[q]);
-        fsm[c * Nk + k] = acc;
+        double acc = I.raw[row * 3 * Nk + it];
+        for (int pt = 1; pt < IN_PARTS; ++pt) acc += I.raw[(pt * rows + row) * 3 * Nk + it];
+        fsm[it] = acc;
     }
     __syncthreads();
     for (int c = 0; c < 3; ++c) {
@@ -259,16 +290,17 @@ __global__ void __launch_bounds__(IN_NT) inflow_kernel(const __grid_constant__ I
     for (int k = threadIdx.x; k < Nk; k += IN_NT) {
         const long long idx = ((long long)gi * Nj + j) * Nk + k;
         const double y = B.met[WM_MET_XCY * N + idx] / I.L;
-        const double uu = fmax(interp_col(I.table, I.n_tab, y, 3), 0.0) * (U * U);
-        const double vv = fmax(interp_col(I.table, I.n_tab, y, 4), 0.0) * (U * U);
-        const double ww = fmax(interp_col(I.table, I.n_tab, y, 5), 0.0) * (U * U);
-        const double uv = interp_col(I.table, I.n_tab, y, 6) * (U * U);
+        const InterpAt at(I.table, I.n_tab, y);
+        const double uu = fmax(at.col(I.table, y, 3), 0.0) * (U * U);
+        const double vv = fmax(at.col(I.table, y, 4), 0.0) * (U * U);
+        const double ww = fmax(at.col(I.table, y, 5), 0.0) * (U * U);
+        const double uv = at.col(I.table, y, 6) * (U * U);
         const double su = sqrt(uu);
         const double l10 = su > 1e-14 ? uv / fmax(su, 1e-14) : 0.0;
         const double l11 = sqrt(fmax(vv - l10 * l10, 0.0));
         const double n0 = fsm[k], n1 = fsm[Nk + k], n2 = fsm[2 * Nk + k];
-        const double u = U * interp_col(I.table, I.n_tab, y, 1) + su * n0;
-        const double v = U * interp_col(I.table, I.n_tab, y, 2) + l10 * n0 + l11 * n1;
+        const double u = U * at.col(I.table, y, 1) + su * n0;
+        const double v = U * at.col(I.table, y, 2) + l10 * n0 + l11 * n1;
         const double w = sqrt(ww) * n2;
         const double rho = I.rho_inf, p = I.p_inf;
         I.out[idx] = rho;
@@ -280,6 +312,10 @@ __global__ void __launch_bounds__(IN_NT) inflow_kernel(const __grid_constant__ I
 }
 
 cudaError_t launch_inflow(const InflowArgs& I, int Nj, int Nk, int ng, cudaStream_t s) {
+    const long long units = (long long)IN_PARTS * ng * Nj * 3 * Nk;
+    inflow_modes_kernel<<<(unsigned)((units + IN_NT - 1) / IN_NT), IN_NT, 0, s>>>(I, units);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
     dim3 grid(Nj, ng);
     const size_t sm = sizeof(double) * 3 * Nk;
     inflow_kernel<<<grid, IN_NT, sm, s>>>(I);

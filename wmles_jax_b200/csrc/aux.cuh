@@ -61,8 +61,14 @@ struct InflowArgs {
     double U_inf, L, rho_inf, p_inf, gm1;
     double time0, time_dt;   // time = time0 + time_dt * (*dt)
     const double* dt;
+    double* raw;             // IN_PARTS x (ng * Nj) x 3 x Nk partial mode sums (scratch)
     double* out;             // 5 x (ng * Nj * Nk)
 };
+
+// partial mode sums per (component, cell) of the synthetic inflow (contiguous mode ranges)
+constexpr int IN_PARTS = 4;
+// kernel launches of one inflow fill
+constexpr int IN_LAUNCHES = 2;
 
 // before each stage kernel: ghost gather (single phase), wall model and sponge means in one
 // launch; the CTA counts are filled in by the launcher (an empty part has none)

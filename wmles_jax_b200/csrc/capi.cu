@@ -153,7 +153,7 @@ struct wm_case {
     double* d_bc = nullptr;
     bool has_inflow = false;
     int inflow_block = -1;
-    double *d_modes = nullptr, *d_table = nullptr, *inflow_buf = nullptr;
+    double *d_modes = nullptr, *d_table = nullptr, *inflow_buf = nullptr, *inflow_raw = nullptr;
     wm_inflow inflow{};
     long long inflow_n = 0;
     std::vector<double*> spmean;         // per block, null without sponge
@@ -432,8 +432,9 @@ int fill_inflow(View* v, Prof* pf, const double* times, double time_dt, const do
         I.U_inf = c->inflow.U_inf; I.L = c->inflow.L; I.rho_inf = c->inflow.rho_inf; I.p_inf = c->inflow.p_inf;
         I.gm1 = c->hc.gm1;
         I.time0 = times[ci]; I.time_dt = time_dt; I.dt = dt ? dt[ci] : nullptr;
+        I.raw = c->inflow_raw;
         I.out = c->inflow_buf;
-        LaunchScope ls(pf, WM_KIND_SOURCE, s);
+        LaunchScope ls(pf, WM_KIND_SOURCE, s, IN_LAUNCHES);
         CK(launch_inflow(I, B.N[1], B.N[2], B.ng, s));
     }
     return WM_OK;
@@ -674,6 +675,7 @@ int wm_case_create(const wm_case_desc* d, wm_case** out) {
         const BlockDev& B = c->hb[I.block];
         c->inflow_n = (long long)B.ng * B.plane;
         if ((r = c->mem.alloc(&c->inflow_buf, 5 * (size_t)c->inflow_n))) return bail(r);
+        if ((r = c->mem.alloc(&c->inflow_raw, (size_t)IN_PARTS * 3 * c->inflow_n))) return bail(r);
     }
 
     // ---- sponge means
@@ -866,7 +868,7 @@ int wm_batch_info(wm_batch* b, int* nblocks, int* ntiles, long long* launches_pe
     const View& v = b->view;
     int inflow = 0;
     for (wm_case* c : v.members) inflow += c->has_inflow ? 1 : 0;
-    const long long per_stage = inflow + ((v.total_rhs || !v.hw.empty() || v.any_sponge) ? 1 : 0) + 1;
+    const long long per_stage = IN_LAUNCHES * inflow + ((v.total_rhs || !v.hw.empty() || v.any_sponge) ? 1 : 0) + 1;
     if (nblocks) *nblocks = v.nblocks;
     if (ntiles) *ntiles = (int)v.tiles.size();
     if (launches_per_step) *launches_per_step = 3 * per_stage + 1;
