@@ -308,7 +308,7 @@ def run_ours(args, rank, world, local_rank):
         line["cpu_baseline"] = cpu_baseline(args.cpu_cells)
     if world == 1 and args.extra:
         line["diagnostics"] = diagnostics_leg(mesh, s64, Q64, cells)
-        del s64, s32, Q64, Q32, Qn, dbuf
+        del s64, s32, Q64, Q32, dbuf, pin_in, pin_out
         line["mixed"]["error_vs_fp64"] = precision_leg()
         line["configs"] = configs_leg()
     if world == 1 and args.serving_requests > 0:
