@@ -80,7 +80,7 @@ def test_golden_case(W, golden, tag):
 
 
 def test_cfg1_channel_100_steps_matches_reference(W, golden_cfg1):
-    """North-star parity bar: FP64 step within 1e-10 relative L2 of the reference after
+    """The FP64 parity bar: FP64 step within 1e-10 relative L2 of the reference after
     100 steps of the config-1 channel (2 blocks of 16x32x16, KEP2, Smagorinsky, wall model,
     constant mass flux)."""
     mesh, gas, kw, prim = C.cfg1_case(W)

@@ -24,7 +24,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relax
           "-I", os.path.join(HERE, "..", "include")]
 # stage.cu: single-precision division and square root without IEEE rounding and with
 # denormals flushed.  These options act on FP32 operations only: the FP64 stage kernels are
-# unchanged, and the mixed form's FP32 fluxes, gradients and SGS are judged against FP64
+# unchanged, and the mixed form's FP32 fluxes, gradients and SGS are compared with FP64
 # at a tolerance far above the last-place error of these instructions.
 PER_FILE = {"surface.cu": ["-fmad=false"], "geom.cu": ["-fmad=false"],
             "stage.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]}

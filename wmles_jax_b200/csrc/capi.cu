@@ -253,7 +253,7 @@ int validate(const wm_case_desc* d) {
         return fail(WM_E_UNSUPPORTED, "tile 3 (16x32) is built for the mixed form only");
     for (int b = 0; b < d->nblocks; ++b) {
         const wm_block& B = d->blocks[b];
-        if (B.ng != 3) return fail(WM_E_UNSUPPORTED, "block %d: ng=%d (this build supports ng=3)", b, B.ng);
+        if (B.ng != 3) return fail(WM_E_UNSUPPORTED, "block %d: ng=%d (this library supports ng=3)", b, B.ng);
         for (int a = 0; a < 3; ++a)
             if (B.n[a] < B.ng) return fail(WM_E_INVALID, "block %d: n[%d]=%d < ng", b, a, B.n[a]);
         if (!B.metrics) return fail(WM_E_INVALID, "block %d: null metrics", b);

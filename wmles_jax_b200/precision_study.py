@@ -3,7 +3,7 @@
     python -m wmles_jax_b200.precision_study --config 2 --steps 1000
 
 Both forms start from the same initial state and advance ``steps`` steps, each with its own
-CFL time step (the drivers' loop).  Reported, per result the mixed form is judged on:
+CFL time step (the drivers' loop).  Reported, per result the mixed form is evaluated on:
 
 * state: relative L2 difference of every conservative variable after the last step;
 * mean velocity profile: the velocity averaged over the homogeneous directions (x and z
