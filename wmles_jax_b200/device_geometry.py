@@ -25,11 +25,12 @@ def block_geometry(X):
     NMET x N0 x N1 x N2 float64) of one block from its extended node array X
     (3, N0+1, N1+1, N2+1).  Runs on a private stream and waits for it, so it can run
     beside other device work (e.g. a server's steps on other streams)."""
-    lib = N.load()
-    dev = require_gpu()
+    X = np.asarray(X)
     Nc = tuple(int(s) - 1 for s in X.shape[1:])
-    if len(Nc) != 3 or X.shape[0] != 3 or min(Nc) < 1:
+    if X.ndim != 4 or X.shape[0] != 3 or min(Nc) < 1:
         raise ValueError(f"node array of shape {X.shape}: expected (3, N0+1, N1+1, N2+1)")
+    dev = require_gpu()
+    lib = N.load()
     n = int(np.prod(Nc))
     fext = [tuple(Nc[a] + (a == d) for a in range(3)) for d in range(3)]
     sizes = [n, 3 * n] + [3 * int(np.prod(e)) for e in fext] * 2
