@@ -190,6 +190,31 @@ int wm_step_fused(wm_case* c, double* const* q_in, double* const* q_out, const d
 int wm_max_dt_noalloc(int nblocks, const int* dims, const double* const* q, const double* const* metrics,
                       const wm_gas* gas, double cfl, double* dt_dev, void* stream);
 
+/* Per-case status word (no reference counterpart: the reference only prints rho_min,
+ * examples/channel_wmles.py:141).  The kernels OR these bits into the case's word as they
+ * see the condition; the word keeps them until it is cleared:
+ *   WM_ST_NONFINITE   a NaN or infinite conservative value in a state the CFL / constraint
+ *                     pass reads (a step's output, or the input of wm_max_dt)
+ *   WM_ST_RHO         density <= 0 there
+ *   WM_ST_PRESSURE    pressure <= 0 there
+ *   WM_ST_DT          a CFL time step that is not finite and positive
+ *   WM_ST_WALL        a wall-model Newton solve still moving (relative update > 1e-8) after
+ *                     its n_iter iterations (informational: the reference stops there too)
+ * WM_ST_FATAL = the first four: the state is no longer a flow state. */
+#define WM_ST_NONFINITE 1u
+#define WM_ST_RHO 2u
+#define WM_ST_PRESSURE 4u
+#define WM_ST_DT 8u
+#define WM_ST_WALL 16u
+#define WM_ST_FATAL (WM_ST_NONFINITE | WM_ST_RHO | WM_ST_PRESSURE | WM_ST_DT)
+
+/* Read the case's status word into *status (synchronises `stream`); clear != 0 resets it. */
+int wm_case_status(wm_case* c, unsigned* status, int clear, void* stream);
+
+/* WM_E_NONFINITE (with the bits named in wm_last_error) if the case's status word holds a
+ * WM_ST_FATAL bit, else WM_OK; synchronises `stream` and clears the word. */
+int wm_check(wm_case* c, void* stream);
+
 /* (tau_w, q_w) of every wall-modelled face: out[w] is a device buffer of 2 x nt1 x nt2. */
 int wm_wall_stats(wm_case* c, const double* const* q, double* const* out, void* stream);
 
@@ -239,6 +264,11 @@ int wm_batch_create(int ncases, wm_case* const* cases, wm_batch** out);
 void wm_batch_destroy(wm_batch* b);
 int wm_batch_step(wm_batch* b, double* const* q_in, double* const* q_out, const double* const* dt_in,
                   double* const* dt_next, const double* times, void* stream);
+/* Status words of the batch's member cases, in member order, copied to status (ncases
+ * unsigned, host memory; page-locked memory keeps the copy asynchronous) on `stream`
+ * without waiting: read them after an event recorded behind this call.  The words are not
+ * cleared (their bits only accumulate), so a later read never loses a fault. */
+int wm_batch_status(wm_batch* b, unsigned* status, void* stream);
 /* blocks and stage tiles of the batch, and the number of kernel launches of one step */
 int wm_batch_info(wm_batch* b, int* nblocks, int* ntiles, long long* launches_per_step);
 

@@ -271,6 +271,68 @@ def golden_case(W, tag):
     raise KeyError(tag)
 
 
+def cfg2_small_case(W, n=(32, 32, 16)):
+    """The config-2 channel physics on a reduced grid: one block, tanh stretching beta=2.5,
+    KEP4, WALE Cw=0.5, wall model at the 3rd cell (isothermal), constant mass flux, CFL 0.5;
+    Spalding-law IC with 10 % seeded noise tapered towards the walls (seed 0)."""
+    from wmles_jax_b200.workloads import loglaw_prim
+    gas = channel_gas(W)
+    mesh = channel_case(W, n=n, blocks=1, beta=2.5)
+    kw = dict(scheme=W.KEP(4), sgs="wale", sgs_kwargs=dict(Cw=0.5), cfl=0.5,
+              constraints=[W.ConstantMassFlux(0, 1.0)])
+    return mesh, gas, kw, loglaw_prim(gas, mesh, seed=0)
+
+
+# 100-step trajectories recorded from the reference: (mesh, gas, kw, prim, t0) per case
+TRAJ_CASES = ["cfg2_small", "ramp_small", "naca_small"]
+TRAJ_STEPS = 100
+
+
+def traj_case(W, tag):
+    if tag == "cfg2_small":
+        mesh, gas, kw, prim = cfg2_small_case(W)
+        return mesh, gas, kw, prim, 0.0
+    return golden_case(W, tag)
+
+
+# Sod shock tube of the reference's shock test (tests/test_sod.py:7-28): 100 cells,
+# Extrapolate ends, periodic y/z, R = 1, mu_ref = 1e-9, CFL 0.5, run to t = 0.2
+SOD_NX, SOD_TEND = 100, 0.2
+SOD_SCHEMES = {"muscl": lambda W: W.MUSCLHLLC(), "hybrid": lambda W: W.Hybrid(th0=0.3, th1=0.6)}
+
+
+def sod_run(W, solver_cls, scheme, to_host=np.asarray, init=None, **solver_kw):
+    """Run the Sod tube with the reference's loop (dt = min(max_dt, t_end - t)); returns
+    (mesh, final state, dts).  ``to_host`` turns a state array into NumPy; ``init(solver,
+    prim_fn)`` builds the initial state (default: ``solver.init_state(prim_fn)``)."""
+    mesh = sod_case(W, nx=SOD_NX)
+    gas = W.Gas(R=1.0, mu_ref=1e-9)
+    s = solver_cls(mesh, gas, scheme, sgs=None, cfl=0.5, **solver_kw)
+    Q = init(s, sod_prim) if init else s.init_state(sod_prim)
+    t, dts = 0.0, []
+    while t < SOD_TEND - 1e-12:
+        dt = min(float(s.max_dt(Q)), SOD_TEND - t)
+        Q = s.advance(Q, dt)
+        t += dt
+        dts.append(dt)
+    return mesh, [to_host(q) for q in Q], np.array(dts)
+
+
+# free-stream preservation on the skewed periodic box (tests/test_multiblock.py:100-107):
+# uniform state, every direction periodic, residual bound 0.1 (energy flux scale ~1e7)
+FREESTREAM_PRIM = (1.2, 50.0, -20.0, 30.0, 1e5)
+FREESTREAM_SCHEMES = {"kep2": lambda W: W.KEP(2), "kep4": lambda W: W.KEP(4),
+                      "muscl": lambda W: W.MUSCLHLLC(), "hybrid": lambda W: W.Hybrid()}
+
+
+def freestream_prim(xc):
+    return np.stack([v + 0 * xc[0] for v in FREESTREAM_PRIM])
+
+
+def freestream_mesh(W):
+    return skew_case(W, "single", n=(12, 10, 8), ybc="periodic")
+
+
 def cfg1_case(W):
     """Config-1 channel: 2 blocks of 16x32x16, KEP2, Smagorinsky 0.1, wall model at the 3rd
     cell (isothermal), constant mass flux, CFL 0.5; laminar IC + 5% seeded noise."""

@@ -70,16 +70,71 @@ def record_case(out, tag, mesh, solver, Q, time_=0.0, geom=False, advance=True):
                 out[f"{tag}/xf{d}_{ib}"] = np.asarray(g.xf[d])
 
 
+def make_trajectories(W, C):
+    """golden_traj.npz: the reference's own trajectories, run here.
+
+    * <case>/...: 100 steps of the reduced config-2 channel (KEP4 + WALE + wall model +
+      constant mass flux), the small smooth ramp (Hybrid + Vreman + synthetic inflow +
+      sponge + characteristic outflow) and the NACA C-grid at 1/8 of its cell counts, with
+      the drivers' loop (dt = max_dt(Q, t); Q = advance(Q, dt, t); t += dt): every dt, the
+      final interior state, the final wall stress, and the initial state's checksums.
+    * sod/<scheme>/...: the reference's Sod tube (tests/test_sod.py:7-28) run to t = 0.2 with
+      MUSCL-HLLC and with Hybrid (th0 0.3, th1 0.6): the final interior state and the dts.
+    * freestream/<scheme>: the reference's free-stream residual on the skewed periodic box
+      (tests/test_multiblock.py:100-107), max over variables of max |RHS|.
+    """
+    out = {}
+    for tag in C.TRAJ_CASES:
+        mesh, gas, kw, prim, t = C.traj_case(W, tag)
+        solver = W.Solver(mesh, gas, **kw)
+        Q = solver.init_state(prim)
+        out[f"{tag}/ic_sum"] = np.array([[float(np.sum(np.asarray(q)[v])) for v in range(5)] for q in Q])
+        out[f"{tag}/t0"] = np.array(t)
+        t0 = time.perf_counter()
+        dts = []
+        for _ in range(C.TRAJ_STEPS):
+            dt = float(solver.max_dt(Q, t))
+            Q = solver.advance(Q, dt, t)
+            t += dt
+            dts.append(dt)
+        out[f"{tag}/dts"] = np.array(dts)
+        for ib, (blk, q) in enumerate(zip(solver.blocks, Q)):
+            out[f"{tag}/final{ib}"] = interior(blk, np.asarray(q))
+        for (bname, face), (tau, qw) in sorted(solver.wall_stats(Q).items()):
+            out[f"{tag}/tau/{bname}/{face}"] = np.asarray(tau)
+        print(f"trajectory {tag}: {C.TRAJ_STEPS} steps, {time.perf_counter() - t0:.1f} s")
+    for name, make in C.SOD_SCHEMES.items():
+        mesh, Q, dts = C.sod_run(W, W.Solver, make(W))
+        out[f"sod/{name}/final"] = interior(mesh.blocks[0], Q[0])
+        out[f"sod/{name}/dts"] = dts
+        print(f"sod {name}: {len(dts)} steps")
+    for name, make in C.FREESTREAM_SCHEMES.items():
+        mesh = C.freestream_mesh(W)
+        s = W.Solver(mesh, W.Gas(), make(W), sgs="vreman", cfl=0.5)
+        R = s.rhs(s.init_state(C.freestream_prim))
+        out[f"freestream/{name}"] = np.array(max(float(np.abs(interior(mesh.blocks[0], np.asarray(R[0]))[v]).max())
+                                                for v in range(5)))
+        print(f"free stream {name}: residual {float(out[f'freestream/{name}']):.3e}")
+    np.savez_compressed(os.path.join(HERE, "golden_traj.npz"), **out)
+    print("wrote golden_traj.npz:", len(out), "arrays")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--skip-cfg1", action="store_true", help="keep the existing config-1 fixture")
+    ap.add_argument("--traj-only", action="store_true",
+                    help="write only golden_traj.npz (100-step trajectories, Sod, free stream)")
     args = ap.parse_args()
     W = load_reference(args.reference)
     sys.path.insert(0, HERE)
     sys.path.append(ROOT)
     import cases as C
+
+    make_trajectories(W, C)
+    if args.traj_only:
+        return
 
     # ---------------------------------------------------------------- small topology/physics cases
     out = {}

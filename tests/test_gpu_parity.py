@@ -189,3 +189,29 @@ def test_bad_state_rejected(W):
         gpu.rhs(tuple(torch.zeros((5, 4, 4, 4), dtype=torch.float64, device="cuda") for _ in mesh.blocks))
     with pytest.raises(TypeError):
         gpu.rhs(tuple(torch.zeros((5,) + b.N, dtype=torch.float64) for b in mesh.blocks))
+
+
+@pytest.mark.parametrize("tag", ["split_wm_hybrid", "channel_small_cmf"])
+def test_output_ghost_cells_defined(W, golden, tag):
+    """Ghost cells of a returned state: the input's (after the step's boundary fill) plus
+    the constraint's shift, never uninitialised memory."""
+    mesh, gas, kw, prim, t = C.golden_case(W, tag)
+    nb = len(mesh.blocks)
+    gpu = _solver(mesh, gas, kw)
+    for path in ("advance", "step"):
+        Q = _dev(tuple(golden[f"{tag}/q{ib}"] for ib in range(nb)))
+        # poison the memory the outputs will come from
+        junk = [torch.full_like(q, float("nan")) for q in Q]
+        del junk
+        Q1 = gpu.advance(Q, gpu.max_dt(Q), t) if path == "advance" else gpu.step(Q, t)[0]
+        for blk, q, q1 in zip(mesh.blocks, Q, Q1):
+            ghost = torch.ones(q.shape[1:], dtype=torch.bool, device=q.device)
+            blk.interior(ghost)[...] = False
+            a, b = q[:, ghost], q1[:, ghost]
+            assert bool(torch.isfinite(b).all())
+            if "cmf" in tag:
+                shift = b[1] - a[1]                 # uniform momentum shift of the constraint
+                assert float((shift - shift[0]).abs().max()) <= 1e-12 * float(a[1].abs().max())
+                assert torch.equal(b[0], a[0]) and torch.equal(b[2:4], a[2:4])
+            else:
+                assert torch.equal(a, b)

@@ -144,3 +144,65 @@ def test_server_survives_a_failing_request():
     assert not results[98].ok and "memory" in results[98].error
     _check_server({k: v for k, v in results.items() if k not in (98, 99)}, reqs[:2], alone)
     assert srv.stats["failed"] == 2 and srv.stats["nonfinite"] == 0
+
+
+def _poisoned(req, value, var):
+    """The request with one interior cell of its initial condition replaced by ``value``
+    in primitive variable ``var`` (a host-side fault: NaN, or a negative pressure)."""
+    from wmles_jax_b200.serving import Request
+    build = req.build
+
+    def poisoned():
+        mesh, gas, kw, prim = build()
+
+        def prim2(xc):
+            w = prim(xc)
+            c = tuple(s // 2 for s in w.shape[1:])
+            w[(var,) + c] = value
+            return w
+        return mesh, gas, kw, prim2
+    return Request(rid=req.rid, build=poisoned, steps=req.steps, arrival=req.arrival, dims=req.dims)
+
+
+@pytest.mark.parametrize("value,var,bit", [(float("nan"), 1, 1), (-5.0e3, 4, 4)])
+def test_server_evicts_a_faulted_case(value, var, bit):
+    """A request whose initial state holds a NaN velocity or a negative pressure is evicted
+    with an error naming the fault; the other requests finish bit-identical to running alone;
+    Solver.check raises on the same case run alone."""
+    from wmles_jax_b200 import Solver, _native as N
+    from wmles_jax_b200.serving import Server, serve_alone
+    reqs = _requests([12, 20, 7, 15], [0.0, 0.0, 0.2, 0.4])
+    bad = 1
+    reqs[bad] = _poisoned(reqs[bad], value, var)
+    alone = {r.rid: serve_alone(r) for r in reqs if r.rid != bad}
+    srv = Server(precision="mixed", graphs=True, graph_after=1)
+    results = srv.run(reqs, timeout=300)
+    assert sorted(results) == [r.rid for r in reqs]
+    res = results[bad]
+    assert not res.ok and res.state is None and "NonFiniteStateError" in res.error, res.error
+    assert N.ST_NAMES[bit] in res.error
+    assert srv.stats["evicted"] == 1 and srv.stats["failed"] == 1
+    for r in reqs:
+        if r.rid == bad:
+            continue
+        Q, dt = alone[r.rid]
+        assert results[r.rid].ok and _same(results[r.rid].state, Q) and torch.equal(results[r.rid].dt, dt)
+    mesh, gas, kw, prim = reqs[bad].build()
+    s = Solver(mesh, gas, precision="mixed", **kw)
+    Q, _ = s.step(s.init_state(prim))
+    assert s.status() & bit
+    with pytest.raises(N.NonFiniteStateError):
+        s.check()
+    assert s.status() == 0                      # check() cleared the word
+
+
+def test_status_clean_on_a_healthy_case():
+    from wmles_jax_b200 import Solver, _native as N
+    reqs = _requests([3], [0.0])
+    mesh, gas, kw, prim = reqs[0].build()
+    s = Solver(mesh, gas, **kw)
+    Q = s.init_state(prim)
+    for _ in range(3):
+        Q, _ = s.step(Q)
+    assert s.status() & N.ST_FATAL == 0
+    s.check()

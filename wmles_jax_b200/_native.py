@@ -72,6 +72,8 @@ SIGNATURES = {
     "wm_step_fused": (C.c_int, [C.c_void_p, PP, PP, c_double_p, c_double_p, C.c_double, C.c_void_p]),
     "wm_max_dt_noalloc": (C.c_int, [C.c_int, c_int_p, PP, PP, C.POINTER(WmGas), C.c_double, c_double_p,
                                     C.c_void_p]),
+    "wm_case_status": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint), C.c_int, C.c_void_p]),
+    "wm_check": (C.c_int, [C.c_void_p, C.c_void_p]),
     "wm_wall_stats": (C.c_int, [C.c_void_p, PP, PP, C.c_void_p]),
     "wm_plane_stats": (C.c_int, [C.c_void_p, C.c_int, c_double_p, c_double_p, C.c_void_p]),
     "wm_derived_fields": (C.c_int, [C.c_void_p, PP, PP, C.c_void_p]),
@@ -80,11 +82,26 @@ SIGNATURES = {
     "wm_batch_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     "wm_batch_destroy": (None, [C.c_void_p]),
     "wm_batch_step": (C.c_int, [C.c_void_p, PP, PP, PP, PP, c_double_p, C.c_void_p]),
+    "wm_batch_status": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "wm_batch_info": (C.c_int, [C.c_void_p, c_int_p, c_int_p, C.POINTER(C.c_longlong)]),
     "wm_profile_enable": (C.c_int, [C.c_void_p, C.c_int]),
     "wm_profile_read": (C.c_int, [C.c_void_p, C.c_int, c_double_p, C.POINTER(C.c_longlong)]),
 }
 KIND_STAGE, KIND_GHOST, KIND_WALL, KIND_DT, KIND_SOURCE = range(5)
+# case status bits (WM_ST_*)
+ST_NONFINITE, ST_RHO, ST_PRESSURE, ST_DT, ST_WALL = 1, 2, 4, 8, 16
+ST_FATAL = ST_NONFINITE | ST_RHO | ST_PRESSURE | ST_DT
+ST_NAMES = {ST_NONFINITE: "non-finite state", ST_RHO: "non-positive density", ST_PRESSURE: "non-positive pressure",
+            ST_DT: "non-finite or non-positive time step", ST_WALL: "wall-model Newton not settled"}
+
+
+def status_names(bits):
+    """Names of the WM_ST_* bits set in ``bits``."""
+    return [name for bit, name in ST_NAMES.items() if bits & bit]
+
+
+class NonFiniteStateError(RuntimeError):
+    """A case's state stopped being a flow state (a WM_ST_FATAL bit of its status word)."""
 NDERIVED = 11
 
 _lib = None
@@ -112,7 +129,7 @@ def load(path=LIB_PATH):
 def check(status, what):
     if status != 0:
         msg = _lib.wm_last_error().decode(errors="replace") if _lib is not None else ""
-        exc = ValueError if status in (-1, -4) else RuntimeError
+        exc = ValueError if status in (-1, -4) else NonFiniteStateError if status == -3 else RuntimeError
         raise exc(f"{what} failed (status {status}): {msg}")
 
 

@@ -108,7 +108,7 @@ def tune(cases, precision="mixed", tiles=None, steps=20, warmup=3, use_cache=Tru
         prepared.append(s)
         if prim is None:
             prim = _uniform_prim(gas)
-        q0.append([np.ascontiguousarray(gas.prim_to_cons(np.asarray(prim(g.xc), float))) for g in s.geoms])
+        q0.append([np.ascontiguousarray(gas.prim_to_cons(np.asarray(prim(g.xc), float))) for g in s.host_geoms])
     timings = {}
     for tile in tiles:
         solvers = []

@@ -1,14 +1,20 @@
-"""Backend selection for the B200 build (cf. wmles/backend.py:18-56).
+"""Backend module of the B200 build (cf. wmles/backend.py:1-76).
 
-``WMLES_BACKEND=cuda`` selects this package's CUDA path.  There is no fallback: the
-solver raises if the CUDA library cannot be loaded or no GPU is visible.
-``WMLES_DEVICE`` keeps the reference's accepted values (auto, cpu, gpu, cuda); ``cpu`` is
-rejected for the cuda backend because this path has no CPU implementation.
-Host-side set-up (meshes, initial conditions) uses NumPy, exposed as ``xp``.
+This package is the ``WMLES_BACKEND=cuda`` path.  The variable is read at import, like the
+reference reads it (wmles/backend.py:10): unset, empty or ``cuda`` select this path; any
+other value (``numpy``, ``jax``) asks for one of the reference's own paths, which this
+package does not implement, so constructing a ``Solver`` then raises instead of running on
+the GPU.  There is no fallback either way: the solver raises if the CUDA library cannot be
+loaded or no GPU is visible.  ``WMLES_DEVICE`` keeps the reference's accepted values (auto,
+cpu, gpu, cuda); ``cpu`` is rejected because this path has no CPU implementation.
+
+``xp`` works on host arrays (NumPy, bit for bit) and on device states (torch), see
+``arrays.py``; ``set_at``, ``jit`` and ``fori_loop`` keep the reference's helpers for case
+code that calls them (wmles/backend.py:57-76).
 """
 import os
 
-import numpy as xp  # noqa: F401  (host-side array namespace for set-up code)
+from .arrays import xp  # noqa: F401
 
 BACKEND = os.environ.get("WMLES_BACKEND", "cuda").strip().lower() or "cuda"
 DEVICE_REQUEST = os.environ.get("WMLES_DEVICE", "auto").strip().lower()
@@ -18,7 +24,11 @@ HAS_JAX = False
 
 
 def require_gpu():
-    """Raise unless a CUDA device is usable; returns the torch device."""
+    """Raise unless this path is selected and a CUDA device is usable; returns the torch
+    device."""
+    if BACKEND != "cuda":
+        raise RuntimeError(f"WMLES_BACKEND={BACKEND} selects the reference's own array path; "
+                           "wmles_jax_b200 implements WMLES_BACKEND=cuda only")
     if DEVICE_REQUEST == "cpu":
         raise RuntimeError("WMLES_DEVICE=cpu: the cuda backend has no CPU path")
     import torch
@@ -43,6 +53,27 @@ def asarray(value, dtype=None):
     places arrays on the JAX device); NumPy dtype semantics for ``dtype``."""
     import torch
     return torch.from_numpy(xp.ascontiguousarray(xp.asarray(value, dtype=dtype))).to(require_gpu())
+
+
+def set_at(a, idx, v):
+    """Functional ``a[idx] = v`` (a new array, wmles/backend.py:57-63) for NumPy arrays and
+    torch tensors."""
+    a = a.clone() if hasattr(a, "clone") else a.copy()
+    a[idx] = v
+    return a
+
+
+def jit(fn, **kw):
+    """No tracing compiler on this path: the step runs as CUDA kernels (wmles/backend.py:66)."""
+    return fn
+
+
+def fori_loop(lo, hi, body, init):
+    """wmles/backend.py:70-76 without JAX: a plain loop."""
+    x = init
+    for i in range(lo, hi):
+        x = body(i, x)
+    return x
 
 
 def __getattr__(name):

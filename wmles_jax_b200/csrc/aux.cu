@@ -122,11 +122,22 @@ __global__ void __launch_bounds__(DT_NT) dt_kernel(const __grid_constant__ DtArg
                 q[m * N + idx] = qv[m];
                 q[4 * N + idx] = qv[4];
             }
+            const double rho = qv[0];
+            const double ir = 1.0 / rho;
+            const double u = qv[1] * ir, v = qv[2] * ir, w = qv[3] * ir;
+            const double p = C.gm1 * (qv[4] - 0.5 * rho * ((u * u + v * v) + w * w));
+            {
+                // the state must still be a flow state (bits kept in the case's status word)
+                unsigned bad = 0u;
+#pragma unroll
+                for (int x = 0; x < 5; ++x)
+                    if (!isfinite(qv[x])) bad = WM_ST_NONFINITE;
+                if (!(rho > 0.0)) bad |= WM_ST_RHO;
+                if (!(p > 0.0)) bad |= WM_ST_PRESSURE;
+                if (bad) atomicOr(C.status, bad);
+            }
             if (D.want_dt) {
-                const double rho = qv[0];
-                const double ir = 1.0 / rho, ivol = 1.0 / vol;
-                const double u = qv[1] * ir, v = qv[2] * ir, w = qv[3] * ir;
-                const double p = C.gm1 * (qv[4] - 0.5 * rho * ((u * u + v * v) + w * w));
+                const double ivol = 1.0 / vol;
                 const double T = p * ir * C.inv_Rg;
                 const double cs = sqrt(C.gamma * C.Rg * T);
                 const double nu = C.nu_fac * sutherland_d(T, C) * ir;
@@ -144,6 +155,38 @@ __global__ void __launch_bounds__(DT_NT) dt_kernel(const __grid_constant__ DtArg
             }
         }
     }
+#pragma unroll 1
+    for (int chunk = blockIdx.x; chunk < D.ngcta; chunk += gridDim.x) {
+        int b = 0;
+        {
+            int hi = D.nblocks - 1;
+            while (b < hi) {
+                const int mid = (b + hi + 1) >> 1;
+                if (D.gcta_start[mid] <= chunk) b = mid; else hi = mid - 1;
+            }
+        }
+        const BlockDev& B = D.blocks[b];
+        const long long g = (long long)(chunk - D.gcta_start[b]) * DT_NT + threadIdx.x;
+        if (g < ghost_cells(B)) {
+            const CaseDev& C = D.cases[B.case_id];
+            const long long N = B.ncell, idx = ghost_cell_index(B, g);
+            const double* src = D.q_src[b];
+            double* q = D.q[b];
+            double qv[5];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) qv[v] = src[v * N + idx];
+            if (D.cmf_delta != nullptr && C.cmf_dir >= 0) {
+                // the reference shifts every cell, ghost cells included (wmles/solver.py:30-36)
+                const double delta = D.cmf_delta[B.case_id];
+                const int m = 1 + C.cmf_dir;
+                const double dE = (2.0 * qv[m] * delta + delta * delta) / (2.0 * qv[0]);
+                qv[m] = qv[m] + delta;
+                qv[4] = qv[4] + dE;
+            }
+#pragma unroll
+            for (int v = 0; v < 5; ++v) q[v * N + idx] = qv[v];
+        }
+    }
     if (!D.want_dt) return;
     if (cur >= 0) flush();
     __syncthreads();
@@ -158,11 +201,23 @@ __global__ void __launch_bounds__(DT_NT) dt_kernel(const __grid_constant__ DtArg
         for (int c = threadIdx.x; c < D.ncases; c += DT_NT) {
             volatile unsigned long long* kp = D.dt_key + c;
             const unsigned long long key = *kp;
-            if (D.dt_out[c] != nullptr) D.dt_out[c][0] = dt_value_of(key);
+            const double dt = dt_value_of(key);
+            if (D.dt_out[c] != nullptr) D.dt_out[c][0] = dt;
+            if (!(dt > 0.0 && dt <= DBL_MAX)) atomicOr(D.cases[c].status, WM_ST_DT);
             *kp = DT_KEY_EMPTY;
         }
         if (threadIdx.x == 0) *D.counter = 0u;
     }
+}
+
+// status words of a batch's member cases into one array (wm_batch_status)
+__global__ void status_gather_kernel(const CaseDev* cases, int ncases, unsigned* out) {
+    for (int c = threadIdx.x; c < ncases; c += blockDim.x) out[c] = *(volatile unsigned*)cases[c].status;
+}
+
+cudaError_t launch_status_gather(const CaseDev* cases, int ncases, unsigned* out, cudaStream_t s) {
+    status_gather_kernel<<<1, 128, 0, s>>>(cases, ncases, out);
+    return cudaGetLastError();
 }
 
 // resident CTAs of one wave of dt_kernel<M> (computed once per process and metric type)
@@ -181,9 +236,9 @@ static int dt_wave() {
 
 cudaError_t launch_dt(const DtArgs& D, cudaStream_t s) {
     if (D.met32)
-        dt_kernel<float><<<std::min(D.ncta, dt_wave<float>()), DT_NT, 0, s>>>(D);
+        dt_kernel<float><<<std::max(1, std::min(std::max(D.ncta, D.ngcta), dt_wave<float>())), DT_NT, 0, s>>>(D);
     else
-        dt_kernel<double><<<std::min(D.ncta, dt_wave<double>()), DT_NT, 0, s>>>(D);
+        dt_kernel<double><<<std::max(1, std::min(std::max(D.ncta, D.ngcta), dt_wave<double>())), DT_NT, 0, s>>>(D);
     return cudaGetLastError();
 }
 

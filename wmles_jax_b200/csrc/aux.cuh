@@ -33,6 +33,12 @@ struct DtArgs {
     int ncases;
     int case_block_start[MAX_CASES + 1];   // blocks of case c: [start[c], start[c+1])
     double* q[WM_MAX_BLOCKS];      // state (modified in place when the constraint is applied)
+    // ghost cells of q (a step's output): set to those of q_src (the step's input, as its
+    // boundary fill left them) plus the constraint's shift, the reference's RK combination
+    // of ghost values the RHS leaves at zero; ngcta = 0: ghost cells untouched
+    const double* q_src[WM_MAX_BLOCKS];
+    int ngcta;
+    int gcta_start[WM_MAX_BLOCKS + 1];     // ghost-cell chunks of block b
     const double* cmf_delta;       // per case: constant-mass-flux shift from stage 3 (null: none)
     int want_dt;                   // 0: constraint only
     int met32;                     // read the float metric copy (mixed form)
@@ -41,6 +47,40 @@ struct DtArgs {
     unsigned int* counter;         // last-CTA-done counter (reset by the last CTA)
     double* dt_out[MAX_CASES];     // per case: time step
 };
+
+// ghost cells of a block: every cell with an index outside the interior in some direction
+__host__ __device__ inline long long ghost_cells(const BlockDev& B) {
+    return B.ncell - (long long)B.n[0] * B.n[1] * B.n[2];
+}
+
+// flat index of ghost cell g (0 <= g < ghost_cells(B)), enumerated as the ghost planes
+// i < ng, i >= ng + ni (all j, k), then for interior i the ghost rows in j (all k), then for
+// interior (i, j) the ghost cells in k
+__device__ __forceinline__ long long ghost_cell_index(const BlockDev& B, long long g) {
+    const int ng = B.ng, ni = B.n[0], nj = B.n[1], nk = B.n[2], Nj = B.N[1], Nk = B.N[2];
+    const long long a = 2LL * ng * Nj * Nk;
+    if (g < a) {
+        const int p = int(g / ((long long)Nj * Nk));
+        const long long r = g - (long long)p * Nj * Nk;
+        const int i = p < ng ? p : ni + p;
+        return (long long)i * Nj * Nk + r;
+    }
+    g -= a;
+    const long long b = (long long)ni * 2 * ng * Nk;
+    if (g < b) {
+        const int ii = int(g / (2LL * ng * Nk));
+        const int r = int(g - (long long)ii * 2 * ng * Nk);
+        const int p = r / Nk, k = r - p * Nk;
+        const int j = p < ng ? p : nj + p;
+        return ((long long)(ng + ii) * Nj + j) * Nk + k;
+    }
+    g -= b;
+    const long long t = g / (2 * ng);
+    const int p = int(g - t * 2 * ng);
+    const int ii = int(t / nj), jj = int(t - (long long)ii * nj);
+    const int k = p < ng ? p : nk + p;
+    return ((long long)(ng + ii) * Nj + (ng + jj)) * Nk + k;
+}
 
 // key of DBL_MAX, the value of an empty minimum (the reset value of DtArgs::dt_key)
 constexpr unsigned long long DT_KEY_EMPTY = 0xFFEFFFFFFFFFFFFFull;
@@ -97,6 +137,7 @@ cudaError_t launch_ghost(const GhostArgs& G, cudaStream_t s);
 cudaError_t launch_surface(SurfaceArgs& A, int max_sponge_rows, cudaStream_t s);
 cudaError_t launch_wall(const WallArgs& W, cudaStream_t s);
 cudaError_t launch_dt(const DtArgs& D, cudaStream_t s);
+cudaError_t launch_status_gather(const CaseDev* cases, int ncases, unsigned* out, cudaStream_t s);
 cudaError_t launch_sponge_mean(const SpongeArgs& S, int max_rows, cudaStream_t s);
 cudaError_t launch_inflow(const InflowArgs& I, int Nj, int Nk, int ng, cudaStream_t s);
 

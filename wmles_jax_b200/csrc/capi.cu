@@ -160,6 +160,7 @@ struct wm_case {
     double* ps_part = nullptr;           // plane-statistics scratch (PS_NQ x max Nj x PS_CHUNKS)
     unsigned* ps_counter = nullptr;
     View* self = nullptr;                // the case as a view of one case
+    unsigned* d_status = nullptr;        // status word (WM_ST_* bits)
     Prof prof;
     ~wm_case();
 };
@@ -188,6 +189,7 @@ struct View {
     unsigned long long* dt_key = nullptr;   // CFL pass: per-case minimum keys
     unsigned* counters = nullptr;        // [0]: CFL reduction, [1]: constant-mass-flux reduction
     std::vector<int> cta_start;          // CFL pass: first CTA of each view block (+ total)
+    std::vector<int> gcta_start;         // same for the blocks' ghost cells (output ghost fill)
     int max_wall_faces = 0, sponge_rows = 0;
     bool any_sponge = false, any_cmf = false;
     StageOpts opts{};
@@ -396,8 +398,11 @@ int build_view(View* v, wm_case* const* cases, int n) {
     tile_shape(v->opts.tile, &tj, &tk);
     build_tiles(v, tj, tk, choose_chunk(v->hb, v->opts, tj, tk, req));
     v->cta_start.assign(1, 0);                  // one interior cell per thread of the CFL pass
-    for (const BlockDev& B : v->hb)
+    v->gcta_start.assign(1, 0);                 // one ghost cell per thread
+    for (const BlockDev& B : v->hb) {
         v->cta_start.push_back(v->cta_start.back() + (int)(((long long)B.n[0] * B.n[1] * B.n[2] + DT_NT - 1) / DT_NT));
+        v->gcta_start.push_back(v->gcta_start.back() + (int)((ghost_cells(B) + DT_NT - 1) / DT_NT));
+    }
     int r;
     Owner& m = v->mem;
     if ((r = m.upload(&v->d_blocks, v->hb.data(), v->hb.size()))) return r;
@@ -491,11 +496,17 @@ int run_stage(View* v, Prof* pf, int stage, double* const* q_in, const double* c
     return WM_OK;
 }
 
-int run_dt(View* v, Prof* pf, double* const* q, bool apply_cmf, bool want_dt, double* const* dt_out, cudaStream_t s) {
+// the CFL / constraint pass over q; with q_src (a step's input) it also sets the ghost
+// cells of q (the step's output) from q_src's
+int run_dt(View* v, Prof* pf, double* const* q, bool apply_cmf, bool want_dt, double* const* dt_out,
+           const double* const* q_src, cudaStream_t s) {
     DtArgs D{};
     D.blocks = v->d_blocks; D.cases = v->d_cases; D.nblocks = v->nblocks;
     D.ncta = v->cta_start.back();
     for (int b = 0; b <= v->nblocks; ++b) D.cta_start[b] = v->cta_start[b];
+    D.ngcta = q_src ? v->gcta_start.back() : 0;
+    for (int b = 0; b <= v->nblocks; ++b) D.gcta_start[b] = v->gcta_start[b];
+    for (int b = 0; b < v->nblocks; ++b) D.q_src[b] = q_src ? q_src[b] : nullptr;
     D.ncases = v->ncases;
     for (int ci = 0; ci <= v->ncases; ++ci) D.case_block_start[ci] = v->case_block_start[ci];
     for (int b = 0; b < v->nblocks; ++b) D.q[b] = q[b];
@@ -517,8 +528,8 @@ int run_step(View* v, Prof* pf, double* const* q_in, double* const* q_out, doubl
     if ((r = run_stage(v, pf, 1, q_in, q_in, w0, dt, times, 0.0, s))) return r;
     if ((r = run_stage(v, pf, 2, w0, q_in, w1, dt, times, 1.0, s))) return r;
     if ((r = run_stage(v, pf, 3, w1, q_in, q_out, dt, times, 0.5, s))) return r;
-    if (want_next || v->any_cmf) return run_dt(v, pf, q_out, v->any_cmf, want_next, dt_next, s);
-    return WM_OK;
+    // constraint, next time step and the output's ghost cells in one pass
+    return run_dt(v, pf, q_out, v->any_cmf, want_next, dt_next, q_in, s);
 }
 
 }  // namespace
@@ -540,7 +551,20 @@ struct wm_batch {
     View view;
     Prof prof;
     std::vector<double*> w0, w1;     // per view block: the member cases' work states
+    unsigned* d_status = nullptr;    // member cases' status words, gathered (wm_batch_status)
 };
+
+namespace {
+const char* status_names(unsigned st) {
+    static thread_local std::string s;
+    s.clear();
+    const char* names[] = {"non-finite state", "non-positive density", "non-positive pressure",
+                           "non-finite or non-positive time step", "wall-model Newton not settled"};
+    for (int b = 0; b < 5; ++b)
+        if (st & (1u << b)) { if (!s.empty()) s += ", "; s += names[b]; }
+    return s.c_str();
+}
+}  // namespace
 
 extern "C" {
 
@@ -698,6 +722,11 @@ int wm_case_create(const wm_case_desc* d, wm_case** out) {
     if ((r = c->mem.alloc(&c->ps_counter, 1))) return bail(r);
     CKB(cudaMemset(c->ps_counter, 0, sizeof(unsigned)));
 
+    // ---- status word (every view of the case points at it)
+    if ((r = c->mem.alloc(&c->d_status, 1))) return bail(r);
+    CKB(cudaMemset(c->d_status, 0, sizeof(unsigned)));
+    c->hc.status = c->d_status;
+
     c->self = new View();
     wm_case* self_list[1] = {c};
     if ((r = build_view(c->self, self_list, 1))) return bail(r);
@@ -732,7 +761,8 @@ int wm_rhs(wm_case* c, double* const* q, double* const* rr, double time, void* s
 int wm_max_dt(wm_case* c, const double* const* q, double* dt_dev, void* stream) {
     if (!c || !dt_dev) return fail(WM_E_INVALID, "null argument");
     if (int r = check_ptrs((const void* const*)q, c->self->nblocks, "q")) return r;
-    return run_dt(c->self, &c->prof, const_cast<double* const*>(q), false, true, &dt_dev, (cudaStream_t)stream);
+    return run_dt(c->self, &c->prof, const_cast<double* const*>(q), false, true, &dt_dev, nullptr,
+                  (cudaStream_t)stream);
 }
 
 int wm_advance(wm_case* c, double* const* q_in, double* const* q_out, const double* dt_dev, double time,
@@ -757,6 +787,24 @@ int wm_step_fused(wm_case* c, double* const* q_in, double* const* q_out, const d
     if (int r = check_ptrs((const void* const*)q_out, c->self->nblocks, "q_out")) return r;
     return run_step(c->self, &c->prof, q_in, q_out, c->work[0].data(), c->work[1].data(), &dt_in, &dt_next, &time,
                     true, (cudaStream_t)stream);
+}
+
+int wm_case_status(wm_case* c, unsigned* status, int clear, void* stream) {
+    if (!c || !status) return fail(WM_E_INVALID, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned st = 0;
+    CK(cudaMemcpyAsync(&st, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    if (clear) CK(cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), s));
+    CK(cudaStreamSynchronize(s));
+    *status = st;
+    return WM_OK;
+}
+
+int wm_check(wm_case* c, void* stream) {
+    unsigned st = 0;
+    if (int r = wm_case_status(c, &st, 1, stream)) return r;
+    if (st & WM_ST_FATAL) return fail(WM_E_NONFINITE, "case status 0x%x: %s", st, status_names(st));
+    return WM_OK;
 }
 
 int wm_wall_stats(wm_case* c, const double* const* q, double* const* out, void* stream) {
@@ -845,11 +893,20 @@ int wm_batch_create(int ncases, wm_case* const* cases, wm_batch** out) {
             b->w0.push_back(cases[ci]->work[0][k]);
             b->w1.push_back(cases[ci]->work[1][k]);
         }
+    if ((r = b->view.mem.alloc(&b->d_status, (size_t)ncases))) { delete b; return r; }
     *out = b;
     return WM_OK;
 }
 
 void wm_batch_destroy(wm_batch* b) { delete b; }
+
+int wm_batch_status(wm_batch* b, unsigned* status, void* stream) {
+    if (!b || !status) return fail(WM_E_INVALID, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    CK(launch_status_gather(b->view.d_cases, b->view.ncases, b->d_status, s));
+    CK(cudaMemcpyAsync(status, b->d_status, sizeof(unsigned) * b->view.ncases, cudaMemcpyDeviceToHost, s));
+    return WM_OK;
+}
 
 int wm_batch_step(wm_batch* b, double* const* q_in, double* const* q_out, const double* const* dt_in,
                   double* const* dt_next, const double* times, void* stream) {

@@ -223,10 +223,14 @@ __device__ __forceinline__ R ducros(const R g[9]) {
 
 // ------------------------------------------------------------------ wall model (FP64)
 // Spalding's law solved for u+ by safeguarded Newton, wmles/wall_model.py:19-40
+// *moving is set when the iteration ends with an update larger than 1e-8 of the iterate
+// (not settled within n_iter; the reference returns that iterate all the same)
 __device__ __forceinline__ double spalding_utau(double kappa, double ekb, int n_iter, double h, double U,
-                                                double rho_w, double mu_w) {
+                                                double rho_w, double mu_w, bool* moving) {
     const double Reh = h * U * rho_w / mu_w;
     double up = fmin(fmax(sqrt(Reh), 1.0), 25.0);
+    double last = 0.0;
+    *moving = false;
     for (int it = 0; it < n_iter; ++it) {
         const double ku = kappa * up;
         const double ex = exp(ku);
@@ -235,9 +239,11 @@ __device__ __forceinline__ double spalding_utau(double kappa, double ekb, int n_
         const double next = fmin(fmax(up - F / dF, 0.5 * up), 100.0);
         // the update is a fixed function of up: once an iterate repeats exactly, every later
         // one does too, so stopping here returns what all n_iter iterations would
-        if (next == up) break;
+        if (next == up) return U / up;
+        last = next - up;
         up = next;
     }
+    *moving = !(fabs(last) <= 1e-8 * up);
     return U / up;
 }
 

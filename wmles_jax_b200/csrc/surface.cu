@@ -211,7 +211,9 @@ __device__ __forceinline__ void wall_face(const WallArgs& A, int w, long long f)
     const double T_w = W.isothermal ? W.T_wall : T_h + C.Pr13 * (Um * Um) / (2.0 * C.cp);
     const double rho_w = p_h / (C.Rg * T_w);
     const double mu_w = sutherland_d(T_w, C);
-    const double ut = spalding_utau(W.kappa, W.ekb, W.n_iter, h, Um, rho_w, mu_w);
+    bool moving;
+    const double ut = spalding_utau(W.kappa, W.ekb, W.n_iter, h, Um, rho_w, mu_w, &moving);
+    if (moving) atomicOr(C.status, WM_ST_WALL);
     const double tau = rho_w * (ut * ut);
     double qw = 0.0;
     if (W.isothermal) {

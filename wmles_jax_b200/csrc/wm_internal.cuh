@@ -37,6 +37,7 @@ struct CaseDev {
     double cmf_target, cmf_volume;
     int sponge;
     double sp_xs, sp_inv_dx, sp_sigma0, sp_invL;   // sigma = sigma0 * ramp(eta)
+    unsigned int* status;  // the case's status word (WM_ST_* bits, set with atomicOr)
 };
 
 struct WallDev {

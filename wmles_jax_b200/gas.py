@@ -3,13 +3,14 @@
 Mirrors the constructor and formulas of the reference ``Gas`` (wmles/gas.py:10-41):
 conservative layout q = [rho, rho u, rho v, rho w, rho E], primitive layout
 w = [rho, u, v, w, p].  On the cuda backend the per-cell conversions run inside the
-CUDA kernels; the NumPy methods here are used for initial conditions and host-side
-setup only, with the same operation order as the reference so that host results are
-bit-identical.
+CUDA kernels; the methods here serve initial conditions, set-up and driver diagnostics,
+on host NumPy arrays (the same operation order as the reference, so host results are
+bit-identical) or on device tensors (through ``xp``, e.g. ``gas.cons_to_prim(Q[0])`` on a
+state, as tests/test_sod.py:25 does).
 """
 from dataclasses import dataclass
 
-import numpy as np
+from .arrays import xp
 
 
 @dataclass(frozen=True)
@@ -33,21 +34,21 @@ class Gas:
 
     def cons_to_prim(self, q):
         """(5, ...) conservative -> ((5, ...) primitive, T); wmles/gas.py:28-33."""
-        q = np.asarray(q)
+        q = xp.asarray(q)
         rho = q[0]
         vel = q[1:4] / rho
         ke = vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]
         p = (self.gamma - 1.0) * (q[4] - 0.5 * rho * ke)
         T = p / (rho * self.R)
-        return np.concatenate([rho[None], vel, p[None]], axis=0), T
+        return xp.concatenate([rho[None], vel, p[None]], axis=0), T
 
     def prim_to_cons(self, w):
         """(5, ...) primitive -> conservative; wmles/gas.py:35-38."""
-        w = np.asarray(w)
+        w = xp.asarray(w)
         rho, vel, p = w[0], w[1:4], w[4]
         ke = vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]
         E = p / (self.gamma - 1.0) + 0.5 * rho * ke
-        return np.concatenate([rho[None], rho * vel, E[None]], axis=0)
+        return xp.concatenate([rho[None], rho * vel, E[None]], axis=0)
 
     def sound_speed(self, T):
-        return np.sqrt(self.gamma * self.R * np.asarray(T))
+        return xp.sqrt(self.gamma * self.R * xp.asarray(T))

@@ -25,6 +25,10 @@ waiting ones, so requests that arrive while others run join the next step.
   batch is bit-identical to the same case advanced alone with ``Solver.step``.
 * Time-to-result is measured from the request's arrival to the moment the host sees the
   device finish the request's last step (an event per step, at most six steps in flight).
+* Failure: every step also copies the members' status words (non-finite state, density or
+  pressure <= 0, bad time step) to page-locked host memory; when the host sees a fatal bit
+  it evicts that case between steps (its result is an error, its memory is freed) while the
+  others go on unchanged (their reductions never mix with another case's).
 
 No reference counterpart: the reference advances one case per ``Solver`` in a Python loop
 (examples/channel_wmles.py:121-152).
@@ -75,6 +79,17 @@ class Batch:
 
     def step(self, q_in, q_out, dt_in, dt_next, times=None, stream=None):
         self.step_args(self.args(q_in, q_out, dt_in, dt_next, times), stream)
+
+    def status_async(self, stream=None):
+        """Enqueue a copy of the member cases' status words (bits _native.ST_*, member order)
+        into a page-locked host array, returned; read it once an event recorded after this
+        call has completed.  The words only accumulate bits, so a read that races a later
+        copy still sees every fault up to the event."""
+        if getattr(self, "_status", None) is None:
+            self._status = torch.zeros(len(self.solvers), dtype=torch.int32).pin_memory()
+        s = C.c_void_p((stream or torch.cuda.current_stream()).cuda_stream)
+        N.check(self._lib.wm_batch_status(self._h, C.c_void_p(self._status.data_ptr()), s), "wm_batch_status")
+        return self._status
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
@@ -195,6 +210,7 @@ class _Resident:
     parity: int = 0       # bufs[parity] holds the current state
     done: int = 0         # steps completed
     admitted: float = 0.0
+    fault: str = None     # set once the case's status word shows a fatal fault
 
 
 @dataclass
@@ -207,7 +223,8 @@ class Result:
     arrival: float
     admitted: float
     finished: float
-    error: str = None     # why the request could not be served (its case could not be built)
+    error: str = None     # why the request could not be served (its case could not be built,
+                          # or its state stopped being a flow state and it was evicted)
 
     @property
     def ok(self):
@@ -287,7 +304,7 @@ class Server:
         if solver.has_inflow:
             raise NotImplementedError("the server advances cases without a synthetic inflow only")
         # the initial state exactly as Solver.init_state builds it
-        q0 = [np.ascontiguousarray(gas.prim_to_cons(np.asarray(prim(g.xc), float))) for g in solver.geoms]
+        q0 = [np.ascontiguousarray(gas.prim_to_cons(np.asarray(prim(g.xc), float))) for g in solver.host_geoms]
         with self._lock, torch.cuda.stream(bstream):
             solver._create()
             qa = tuple(torch.from_numpy(q).to(self.device) for q in q0)
@@ -403,7 +420,7 @@ class Server:
         batch, args, graphs, run_len = None, {}, {}, 0
         builder_done = False
         n = dict(batch_steps=0, graph_steps=0, captures=0, memberships=0, kernel_launches=0, cell_steps=0,
-                 pauses=0)
+                 pauses=0, evicted=0)
         seg, busy_ms = None, 0.0    # device time of the batch steps, per membership segment
 
         def close_segment():
@@ -429,12 +446,26 @@ class Server:
 
         def stamp(upto):
             while len(pending) > upto:
-                ev, fin = pending.pop(0)
+                ev, fin, status, members = pending.pop(0)
                 ev.synchronize()
                 now = clock()
+                # status words of that step's members (bits only accumulate, so a copy enqueued
+                # by a later step and landing meanwhile only adds faults)
+                for r, bits in zip(members, status.tolist()):
+                    if bits & N.ST_FATAL and r.fault is None:
+                        r.fault = (f"NonFiniteStateError: {', '.join(N.status_names(bits & N.ST_FATAL))} "
+                                   f"within the first {r.done} steps")
+                        n["evicted"] += 1
                 for r in fin:
-                    results[r.req.rid] = Result(r.req.rid, r.bufs[r.parity], r.dts[r.parity], r.done,
-                                                r.req.cells, r.req.arrival, r.admitted, now)
+                    if r.fault is None:
+                        results[r.req.rid] = Result(r.req.rid, r.bufs[r.parity], r.dts[r.parity], r.done,
+                                                    r.req.cells, r.req.arrival, r.admitted, now)
+
+        def evict(rs):
+            now = clock()
+            for r in rs:
+                results[r.req.rid] = Result(r.req.rid, None, None, r.done, r.req.cells, r.req.arrival,
+                                            r.admitted, now, error=r.fault)
 
         def release(rs):
             with self._cond:
@@ -461,7 +492,7 @@ class Server:
                         take(ready.get_nowait())
                     except queue.Empty:
                         break
-                leaving = [r for r in active if r.done >= r.req.steps]
+                leaving = [r for r in active if r.done >= r.req.steps or r.fault]
                 if joined or leaving or (batch is None and resident):
                     for r in joined:
                         if r.req.steps <= 0:
@@ -471,13 +502,20 @@ class Server:
                         else:
                             resident.append(r)
                     joined = []
-                    resident = [r for r in resident if r.done < r.req.steps]
+                    resident = [r for r in resident if r.done < r.req.steps and not r.fault]
                     chosen = self._select(resident)
                     if leaving or [id(r) for r in chosen] != [id(r) for r in active]:
                         # membership change: drain the steps in flight, free the leavers, rebuild
                         close_segment()
                         self.stream.synchronize()
                         stamp(0)
+                        # the drained steps may show more faulted cases: they leave now too
+                        late = [r for r in resident if r.fault]
+                        if late:
+                            resident = [r for r in resident if not r.fault]
+                            chosen = self._select(resident)
+                            leaving += [r for r in late if r not in leaving]
+                        evict([r for r in leaving if r.fault])
                         graphs.clear()
                         args = {}
                         if batch is not None:
@@ -513,6 +551,7 @@ class Server:
                     n["graph_steps"] += 1
                 else:
                     batch.step_args(args[key], self.stream)
+                status = batch.status_async(self.stream)
                 run_len += 1
                 n["batch_steps"] += 1
                 n["kernel_launches"] += batch.launches_per_step
@@ -525,7 +564,7 @@ class Server:
                         fin.append(r)
                 ev = torch.cuda.Event()
                 ev.record(self.stream)
-                pending.append((ev, fin))
+                pending.append((ev, fin, status, list(active)))
                 stamp(self.in_flight)          # bounded number of steps in flight
             close_segment()
             self.stream.synchronize()
@@ -536,6 +575,11 @@ class Server:
             w.join()
         if errors:
             raise errors[0]
+        # faults seen only in the last drain: those cases finished their steps, but their
+        # results are not flow states
+        for r in list(active) + list(resident):
+            if r.fault and results.get(r.req.rid) is not None and results[r.req.rid].ok:
+                evict([r])
         served = [r for r in results.values() if r.ok]
         wall = max((r.finished for r in served), default=0.0)
         ttr = np.array([r.time_to_result for r in served])

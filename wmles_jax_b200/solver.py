@@ -4,9 +4,11 @@ Same constructor and methods as the reference ``Solver`` (wmles/solver.py:39-232
 ``init_state``, ``apply_bcs``, ``rhs``, ``max_dt``, ``advance``, ``wall_stats``,
 ``wall_loads``, plus ``step`` (max_dt + advance in one call, the drivers' loop body).
 The state is a tuple of torch CUDA float64 tensors (5, Ni, Nj, Nk), ghosts included, and
-every call returns new tensors as the reference's functional API does.  Ghost layers of
-the states returned by ``advance``/``step`` are not part of the result (every consumer
-refills them first, as in the reference, where they hold RK combinations of stale values).
+every call returns new tensors as the reference's functional API does.  ``solver.geoms``
+holds the block geometry on the device (torch tensors), as the reference's does (JAX device
+arrays placed by Mesh.finalize), so driver arithmetic such as ``q[1:4] ** 2 / q[0] * g.vol``
+runs on the device; ``solver.host_geoms`` (= ``mesh.geoms``) is the host NumPy copy the
+set-up uses.
 
 Built-in BCs, schemes, SGS models, ``ConstantMassFlux`` and ``SmoothRampSponge`` are
 recognised by class and lowered into one ``wm_case`` of libwmles_cuda.so; anything else
@@ -59,8 +61,8 @@ class Solver:
         device call; a server runs it on a worker thread)."""
         self.device = require_gpu()
         self.mesh, self.blocks, self.gas = mesh, mesh.blocks, gas
-        self.geoms = mesh.geoms
-        if self.geoms is None:
+        self.host_geoms = mesh.geoms
+        if self.host_geoms is None:
             raise ValueError("call mesh.finalize() before building the solver")
         self.scheme, self.cfl = scheme, cfl
         self.sgs = make_sgs(sgs, **(sgs_kwargs or {}))
@@ -82,6 +84,20 @@ class Solver:
         self._case = handle
         if release:
             self._keep = self._desc = None         # host arrays were copied to the device
+
+    @property
+    def geoms(self):
+        """Block geometry (Geom of vol, xc, S, xf) as float64 tensors on the solver's device,
+        copied from the host geometry on first use."""
+        dev = getattr(self, "_dev_geoms", None)
+        if dev is None:
+            from .mesh import Geom
+
+            def t(a):
+                return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(self.device)
+            dev = self._dev_geoms = tuple(Geom(t(g.vol), t(g.xc), tuple(t(x) for x in g.S), tuple(t(x) for x in g.xf))
+                                          for g in self.host_geoms)
+        return dev
 
     def __del__(self):
         h = getattr(self, "_case", None)
@@ -123,13 +139,13 @@ class Solver:
             if not isinstance(c, ConstantMassFlux) or d.cmf_dir >= 0:
                 raise NotImplementedError("cuda backend: supports one ConstantMassFlux constraint")
             den = 0.0
-            for b, geo in zip(self.blocks, self.geoms):
+            for b, geo in zip(self.blocks, self.host_geoms):
                 den = den + np.sum(b.interior(geo.vol))        # wmles/solver.py:26-27
             d.cmf_dir, d.cmf_target, d.cmf_volume = int(c.dir), float(c.target), float(den)
         # blocks
         nb = len(self.blocks)
         blocks = (N.WmBlock * nb)()
-        for ib, (b, geo) in enumerate(zip(self.blocks, self.geoms)):
+        for ib, (b, geo) in enumerate(zip(self.blocks, self.host_geoms)):
             blocks[ib].n = (C.c_int * 3)(*b.n)
             blocks[ib].ng = b.ng
             met = block_metrics(b, geo)
@@ -144,7 +160,7 @@ class Solver:
         d.nblocks, d.blocks = nb, blocks
         # wall-modelled faces
         self.walls = []
-        for ib, (b, geo) in enumerate(zip(self.blocks, self.geoms)):
+        for ib, (b, geo) in enumerate(zip(self.blocks, self.host_geoms)):
             for (a, s), bc in sorted(b.faces.items()):
                 if isinstance(bc, WallModel):
                     self.walls.append((ib, a, s, bc))
@@ -156,7 +172,7 @@ class Solver:
             walls[w].T_wall = 0.0 if bc.T_wall is None else float(bc.T_wall)
             walls[w].kappa, walls[w].B, walls[w].n_iter = float(m.kappa), float(m.B), int(m.n_iter)
             blk = self.blocks[ib]
-            geo = wall_geometry(blk, self.geoms[ib], a, s, bc.n_match)
+            geo = wall_geometry(blk, self.host_geoms[ib], a, s, bc.n_match)
             nt = [blk.n[t] for t in range(3) if t != a]
             if geo.shape != (5, nt[0], nt[1]):
                 raise RuntimeError(f"wall geometry of block {blk.name}: shape {geo.shape}, expected {(5, *nt)}")
@@ -164,7 +180,7 @@ class Solver:
         self._keep.append(walls)
         d.nwalls, d.walls = len(self.walls), walls
         # ghost programs
-        prog_rhs, prog_all, table = lower_ghost_programs(self.blocks, self.geoms, g, self.bc_passes)
+        prog_rhs, prog_all, table = lower_ghost_programs(self.blocks, self.host_geoms, g, self.bc_passes)
         self.ghost_programs = (prog_rhs, prog_all)
         d.ghost_rhs, d.ghost_all = self._program(prog_rhs), self._program(prog_all)
         d.nbc, d.bc_table = len(table), N.as_double_p(self._arr(table, np.float64))
@@ -223,7 +239,7 @@ class Solver:
         """prim_fn(xc) -> primitives [rho, u, v, w, p] at the ghosted cell centres
         (wmles/solver.py:54-56); evaluated with NumPy on the host, then uploaded."""
         out = []
-        for geo in self.geoms:
+        for geo in self.host_geoms:
             w = np.asarray(prim_fn(geo.xc), float)
             out.append(torch.from_numpy(np.ascontiguousarray(self.gas.prim_to_cons(w))).to(self.device))
         return tuple(out)
@@ -254,7 +270,11 @@ class Solver:
         return dt
 
     def advance(self, Q, dt, time=0.0):
-        """One SSP-RK3 step plus constraints (wmles/solver.py:123-133)."""
+        """One SSP-RK3 step plus constraints (wmles/solver.py:123-133).  The interior is the
+        result; the ghost cells of the returned state are those of Q after the step's
+        boundary fill (which refreshes Q's ghost cells in place) plus the constraint's shift,
+        as in the reference, where the RK stages combine ghost values the RHS leaves at
+        zero and the constraint shifts every cell."""
         self._check_state(Q)
         dtt = self._dt_tensor(dt)
         out = tuple(torch.empty_like(q) for q in Q)
@@ -282,6 +302,22 @@ class Solver:
                                         float(time), self._stream()), "wm_step_fused")
         self._chain = (tuple((weakref.ref(q), q._version) for q in out), dt_next)
         return out, dt
+
+    # ------------------------------------------------------------------ failure detection
+    def status(self, clear=False):
+        """The case's status word (bits _native.ST_*: non-finite state, non-positive density
+        or pressure, bad time step, unsettled wall-model Newton), accumulated by the kernels
+        since the last clear; synchronises the current stream."""
+        st = C.c_uint()
+        N.check(self._lib.wm_case_status(self._case, C.byref(st), 1 if clear else 0, self._stream()),
+                "wm_case_status")
+        return st.value
+
+    def check(self):
+        """Raise _native.NonFiniteStateError if a step or CFL pass since the last check saw a
+        state that is no longer a flow state (NaN / Inf, density or pressure <= 0, a time step
+        that is not finite and positive); clears the word.  Synchronises the current stream."""
+        N.check(self._lib.wm_check(self._case, self._stream()), "wm_check")
 
     # ------------------------------------------------------------------ measurement
     def profile(self, enable=True):
@@ -328,7 +364,7 @@ class Solver:
         stats = self.wall_stats(Q)
         out = {}
         for ib, a, s, bc in self.walls:
-            blk, geo = self.blocks[ib], self.geoms[ib]
+            blk, geo = self.blocks[ib], self.host_geoms[ib]
             ng, n = blk.ng, blk.n[a]
             fb = ng if s == 0 else ng + n
             mi = ng + bc.n_match - 1 if s == 0 else ng + n - bc.n_match

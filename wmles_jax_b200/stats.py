@@ -19,7 +19,7 @@ KEYS = ("rho", "u", "v", "w", "uu", "vv", "ww", "uv", "uw", "vw", "T", "p")
 class PlaneStats:
     def __init__(self, mesh, solver):
         self.mesh, self.solver = mesh, solver
-        blk, geom = mesh.blocks[0], solver.geoms[0]
+        blk, geom = mesh.blocks[0], solver.host_geoms[0]
         self.y = np.asarray(blk.interior(geom.xc[1]))[0, :, 0]
         self.n = 0
         self._sum = torch.zeros((len(KEYS), blk.n[1]), dtype=torch.float64, device=solver.device)
