@@ -39,8 +39,8 @@ METRIC = "Mcell-steps/s"
 CONFIG_NAME = "channel 256x128x128, KEP4 + WALE + wall model + constant mass flux, SSP-RK3"
 N_CFG2 = (256, 128, 128)
 # DRAM bytes (read + write) per stage-kernel launch per interior cell, mean of the three RK
-# stages, from one ncu capture of the same kernel on a 128^3 case of this workload
-# (profiles/stage_kernel_channel.md); scaled by the cell count for the roofline's `traffic`
+# stages, from one ncu capture of the same kernel on a 128^3 case of this workload; scaled
+# by the cell count for the roofline's `traffic`
 TRAFFIC_PER_CELL = {"fp64": 321.0, "mixed": 229.0}
 
 

@@ -184,8 +184,10 @@ int wm_step_fused(wm_case* c, double* const* q_in, double* const* q_out, const d
  * WM_NOALLOC_MAX_PARTIALS slots (one per 256 interior cells, so at most
  * WM_NOALLOC_MAX_PARTIALS * 256 interior cells in total; larger inputs are rejected with
  * WM_E_INVALID).  The first call on a device looks the array up (cudaGetSymbolAddress), so
- * make it before any stream capture.  All calls share the array: calls that overlap on the
- * GPU race and must be serialised by the caller. */
+ * make it before any stream capture; the lookup is repeated only if the device's context
+ * has been replaced since (cudaDeviceReset), and a first call after that replacement must
+ * also come before any capture.  All calls share the array: calls that overlap on the GPU
+ * race and must be serialised by the caller. */
 #define WM_NOALLOC_MAX_PARTIALS 32768
 int wm_max_dt_noalloc(int nblocks, const int* dims, const double* const* q, const double* const* metrics,
                       const wm_gas* gas, double cfl, double* dt_dev, void* stream);

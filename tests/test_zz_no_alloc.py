@@ -49,6 +49,18 @@ def test_no_alloc_cfl_matches_allocating_entry_point(W):
         assert np.isfinite(got)
         assert abs(got - want) <= 1e-13 * want, (got, want)
 
+    # the property the entry point exists for: once the first call has loaded the library's
+    # module (and with it the static array), further calls take no device memory
+    ptrs = (N.ptr_array([q.data_ptr() for q in states[1]]), N.ptr_array([m.data_ptr() for m in mets]))
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    for _ in range(5):
+        N.check(lib.wm_max_dt_noalloc(len(mesh.blocks), N.as_int_p(dims), ptrs[0], ptrs[1], C.byref(gas_c),
+                                      float(kw["cfl"]), N.ptr_array([out.data_ptr()])[0], stream), "wm_max_dt_noalloc")
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before, (free_before, free_after)
+
 
 def test_no_alloc_rejects_oversized_input():
     from wmles_jax_b200 import _native as N

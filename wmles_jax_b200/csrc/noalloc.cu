@@ -14,6 +14,7 @@
 // by the caller.
 #include <cstdio>
 #include <mutex>
+#include <cuda.h>              // CUcontext / CUresult types only: the driver calls are looked up
 #include "wm_internal.cuh"
 
 namespace {
@@ -24,8 +25,17 @@ constexpr int kThreads = 256;
 // [0]: done-counter, [1 .. WM_NOALLOC_MAX_PARTIALS]: per-CTA minima (double bit patterns)
 static __device__ __align__(256) unsigned long long g_noalloc_scratch[1 + WM_NOALLOC_MAX_PARTIALS];
 
+// per device: the scratch array's address and the id of the context it was looked up in
+// (a context destroyed by cudaDeviceReset and created again reloads the module, possibly
+// elsewhere, so the address is looked up again when the id changes)
 unsigned long long* g_scratch_addr[kMaxDevices] = {nullptr};
+unsigned long long g_scratch_ctx[kMaxDevices] = {0};
 std::mutex g_scratch_mutex;
+
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+CtxGetCurrentFn g_ctx_current = nullptr;
+CtxGetIdFn g_ctx_id = nullptr;
 
 struct NoAllocArgs {
     int nblocks, total_ctas;
@@ -113,13 +123,35 @@ __global__ void __launch_bounds__(kThreads) cfl_noalloc_kernel(const __grid_cons
 
 int fail(int code, const char* msg) { return wm::set_error(code, msg); }
 
-// device address of the scratch array on the current device, looked up once per device
+// id of the calling thread's current context (0: none current yet), through driver entry
+// points looked up once (the library does not link the driver library itself)
+unsigned long long current_context_id() {
+    if (!g_ctx_current || !g_ctx_id) {
+        cudaDriverEntryPointQueryResult q1, q2;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", (void**)&g_ctx_current, 12000, cudaEnableDefault, &q1) !=
+                cudaSuccess || q1 != cudaDriverEntryPointSuccess ||
+            cudaGetDriverEntryPointByVersion("cuCtxGetId", (void**)&g_ctx_id, 12000, cudaEnableDefault, &q2) !=
+                cudaSuccess || q2 != cudaDriverEntryPointSuccess) {
+            g_ctx_current = nullptr;
+            g_ctx_id = nullptr;
+            return 0;
+        }
+    }
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (g_ctx_current(&ctx) != CUDA_SUCCESS || ctx == nullptr || g_ctx_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// device address of the scratch array on the current device: looked up once per device and
+// context (at the first call, and again after the device's context was replaced)
 int scratch_address(unsigned long long** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
         return fail(WM_E_CUDA, "wm_max_dt_noalloc: no usable current device");
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (g_scratch_addr[dev] == nullptr) {
+    const unsigned long long ctx = current_context_id();
+    if (g_scratch_addr[dev] == nullptr || ctx == 0 || ctx != g_scratch_ctx[dev]) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) {
@@ -128,6 +160,7 @@ int scratch_address(unsigned long long** out) {
             return fail(WM_E_CUDA, m);
         }
         g_scratch_addr[dev] = static_cast<unsigned long long*>(p);
+        g_scratch_ctx[dev] = current_context_id();     // the lookup made the context current
     }
     *out = g_scratch_addr[dev];
     return WM_OK;

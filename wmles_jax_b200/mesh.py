@@ -97,10 +97,10 @@ class Interface:
     """Block-to-block connection seen from the destination block (wmles/mesh.py:77-85)."""
 
     def __init__(self, nb, src_face, mapping, flip, shift):
-        self.nb = nb                  # index of the neighbour (source) block
-        self.src_face = src_face      # (axis, side) on the neighbour
-        self.mapping = mapping        # mapping[A axis] -> B axis
-        self.flip = flip              # flip[A axis] (tangential only)
+        self.nb = nb                  # block the ghost values are copied from
+        self.src_face = src_face      # its connected face, (axis, side)
+        self.mapping = mapping        # axis of that block for each axis of this one
+        self.flip = flip              # per axis of this block: index runs reversed (tangential axes)
         self.shift = np.asarray(shift, float)
 
     def __repr__(self):
@@ -212,8 +212,8 @@ def _match_orientation(A, fa, B, fb, shift):
                 mapping[aA], mapping[tA[0]], mapping[tA[1]] = aB, perm[0], perm[1]
                 flip[tA[0]], flip[tA[1]] = bool(f1), bool(f2)
                 return tuple(mapping), tuple(flip)
-    raise ValueError(f"interface {A.name}{fa} <-> {B.name}{fb}: node planes do not match "
-                     f"(check the shift vector and the block node coordinates)")
+    raise ValueError(f"interface {A.name}{fa} <-> {B.name}{fb}: no axis permutation or flip maps one "
+                     f"face's nodes onto the other's (is the periodic shift right?)")
 
 
 class Mesh:
@@ -247,7 +247,7 @@ class Mesh:
         for b in self.blocks:
             for f in FACE_NAMES.values():
                 if f not in b.faces:
-                    raise KeyError(f"block {b.name}: face {f} has no BC / connection")
+                    raise KeyError(f"block {b.name}: face {f} is neither connected nor given a boundary condition")
             X = np.zeros((3,) + tuple(n + 1 + 2 * ng for n in b.n))
             X[(slice(None),) + tuple(slice(ng, ng + n + 1) for n in b.n)] = b.x_int
             b.X = X
@@ -278,7 +278,8 @@ class Mesh:
                 vol, xc, S, xf = compute_geometry(b.X)
                 b.metrics_dev = None
             if vol.min() <= 0:
-                raise ValueError(f"block {b.name}: non-positive cell volume (left-handed or folded grid)")
+                raise ValueError(f"block {b.name}: a cell volume is zero or negative (the node ordering is "
+                                 f"left-handed, or the grid folds over itself)")
             b.geom = Geom(vol, xc, S, xf)
             geoms.append(b.geom)
         self.geoms = tuple(geoms)

@@ -4,7 +4,7 @@ Spalding's law F(u+) = u+ + e^{-kB}(e^{k u+} - 1 - k u+ - (k u+)^2/2 - (k u+)^3/
 is solved for u+ by ``n_iter`` safeguarded Newton steps (clipped to [0.5 u+, 100],
 start clip(sqrt(Re_h), 1, 25)); the wall heat flux uses Kader's temperature law for an
 isothermal wall, or the recovery temperature with q_w = 0 for an adiabatic wall.
-The solve runs per wall face in FP64 in the CUDA wall kernel (csrc/wall.cu).
+The solve runs per wall face in FP64 in the CUDA wall kernel (``wall_face`` in csrc/surface.cu).
 """
 
 
