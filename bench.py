@@ -42,6 +42,10 @@ N_CFG2 = (256, 128, 128)
 # stages, from one ncu capture of the same kernel on a 128^3 case of this workload; scaled
 # by the cell count for the roofline's `traffic`
 TRAFFIC_PER_CELL = {"fp64": 321.0, "mixed": 229.0}
+# FP64 floating-point operations per interior cell per stage-kernel launch (FP64 form), from
+# the same kind of capture (None until measured for the current kernel)
+FP64_FLOP_PER_CELL = None
+FP64_PEAK_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
 
 
 def peaks():
@@ -176,27 +180,44 @@ def run_ours(args, rank, world, local_rank):
         barrier()
         return Q, ms, clk
 
+    def kernel_split(solver, Q, n):
+        """Mean device time of one launch of each kernel kind over n more steps, CUDA events
+        around every launch (a separate pass: the event pairs are not in the timed steps)."""
+        solver.profile(enable=True)
+        for _ in range(n):
+            Q, _ = solver.step(Q)
+        torch.cuda.synchronize()
+        split = {}
+        for kind, name in ((_native.KIND_STAGE, "stage"), (_native.KIND_GHOST, "surface"), (_native.KIND_DT, "dt")):
+            ms, cnt = solver.profile_read(kind)
+            split[name] = dict(ms_per_launch=ms / max(cnt, 1), launches=cnt)
+        solver.profile(enable=False)
+        return Q, split
+
     out = {}
     s64 = Solver(mesh, gas, **kw)
     Q = tuple(torch.from_numpy(q).to(dev) for q in Q0h)
-    Q64, ms64, clk = timed(s64, Q, profile=True)
-    st_ms, st_n = s64.profile_read(_native.KIND_STAGE)
+    Q64, ms64, clk = timed(s64, Q, profile=False)       # launch counts kept, no event pairs
     all_ms, all_n = s64.profile_read(-1)
     ms64_max = max_over_ranks(ms64)
-    out["fp64"] = dict(ms=ms64_max / K, stage_ms=st_ms / max(st_n, 1), launches=all_n, clk=clk.summary())
+    Q64, split64 = kernel_split(s64, Q64, min(K, 20))
+    out["fp64"] = dict(ms=ms64_max / K, stage_ms=split64["stage"]["ms_per_launch"], launches=all_n,
+                       clk=clk.summary(), split=split64)
 
     # mixed precision form (same workload and IC)
     s32 = Solver(mesh, gas, **kw, precision="mixed")
     Q = tuple(torch.from_numpy(q).to(dev) for q in Q0h)
-    Q32, ms32, clk32 = timed(s32, Q, profile=True)
-    st32_ms, st32_n = s32.profile_read(_native.KIND_STAGE)
+    Q32, ms32, clk32 = timed(s32, Q, profile=False)
     ms32_max = max_over_ranks(ms32)
+    Q32, split32 = kernel_split(s32, Q32, min(K, 20))
+    st32_ms, st32_n = split32["stage"]["ms_per_launch"], 1
     err = []
     for c in range(5):
         a = mesh.blocks[0].interior(Q32[0][c]).double()
         b = mesh.blocks[0].interior(Q64[0][c]).double()
         err.append(float(torch.linalg.norm(a - b) / torch.linalg.norm(b)))
-    out["mixed"] = dict(ms=ms32_max / K, stage_ms=st32_ms / max(st32_n, 1), err=max(err), clk=clk32.summary())
+    out["mixed"] = dict(ms=ms32_max / K, stage_ms=st32_ms / max(st32_n, 1), err=max(err), clk=clk32.summary(),
+                        split=split32)
 
     # end to end through the public API with host buffers.  Each step takes an independent
     # host state (two pinned input buffers, alternating), and its new state goes back to a
@@ -299,11 +320,23 @@ def run_ours(args, rank, world, local_rank):
                      "whole_step_frac": (STEP_BYTES["fp64"] + CMF_BYTES) * cells / (f["ms"] * 1e-3) / 1e9 / hbm},
         "mixed": {"value": cells * world / (out["mixed"]["ms"] * 1e-3) / 1e6, "ms_per_step": out["mixed"]["ms"],
                   "speedup_vs_fp64": f["ms"] / out["mixed"]["ms"],
-                  "state_rel_l2_vs_fp64_after_steps": out["mixed"]["err"], "steps_compared": K + Wm,
-                  "stage_launch_ms": out["mixed"]["stage_ms"],
+                  "state_rel_l2_vs_fp64_after_steps": out["mixed"]["err"], "steps_compared": K + Wm + min(K, 20),
+                  "stage_launch_ms": out["mixed"]["stage_ms"], "kernel_split": out["mixed"]["split"],
                   "roofline_frac": np.mean(STAGE_BYTES["mixed"]) * cells / (out["mixed"]["stage_ms"] * 1e-3) / 1e9 / hbm},
+        "kernel_split": dict(f["split"], how="a separate pass of min(K, 20) steps with CUDA events around every "
+                                              "launch; the timed steps run without them"),
         "clocks": f["clk"],
     }
+    if FP64_FLOP_PER_CELL is not None:
+        # the FP64 stage kernel's other roof: its FP64 instructions against the FP64 pipe
+        fl = FP64_FLOP_PER_CELL * cells
+        tfs = fl / (f["stage_ms"] * 1e-3) / 1e12
+        line["roofline"]["fp64_pipe"] = {
+            "achieved": tfs, "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s", "frac": tfs / FP64_PEAK_TFLOPS,
+            "flop_per_launch": fl, "flop_per_cell": FP64_FLOP_PER_CELL,
+            "flop_source": "ncu: 2 x dfma + dadd + dmul thread instructions per launch (mean of the three "
+                           "RK stages) on a 128^3 case of the workload, per interior cell",
+            "peak_source": "nominal: 148 SMs x 64 FP64 FMA per clock x 2 x 1.965 GHz"}
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.cpu_cells)
     if world == 1 and args.extra:
@@ -461,10 +494,12 @@ def run_reference(args, rank, world):
               f"{n[0]}x{n[1]}x{n[2]} x-periodic slab of the 256x128x128 channel (same physics); "
               f"NumPy float64 oracle restating the reference")
     return {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": slowest / args.steps * 1e3 * (int(np.prod(N_CFG2)) / (
-                cells_steps / args.steps)), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "warmup": args.warmup, "ms_per_step": slowest / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded log-law IC + 10% noise)", "impl": "reference",
-            "config": config_dict({"form": "fp64", "host": "CPU"}),
+            "config": config_dict({"form": "fp64", "host": "CPU",
+                                   "sample_per_process": f"{n[0]}x{n[1]}x{n[2]} slab ({int(np.prod(n))} cells)",
+                                   "ms_per_step": "one step of every process's slab, all processes at once"}),
             "cpu_baseline": {"value": value, "unit": METRIC, "cores": workers, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": wall}

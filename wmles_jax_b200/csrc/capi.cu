@@ -175,6 +175,9 @@ struct View {
     std::vector<CaseDev> hc;
     std::vector<WallDev> hw;
     std::vector<Tile> tiles;             // stage work list: (j,k) columns of every block, cut along i
+    std::vector<int> cta_first;          // balanced split: CTA c runs tiles [cta_first[c], cta_first[c+1])
+                                         // (empty: one tile per CTA)
+    int* d_cta_first = nullptr;
     std::vector<int> case_block_start;
     std::vector<int> cmf_slot_start, case_slot_start;   // constant-mass-flux partial slots
     std::vector<GhostSeg> seg_rhs, seg_all;
@@ -316,12 +319,82 @@ int choose_chunk(const std::vector<BlockDev>& hb, const StageOpts& opts, int tj,
     return best_ic;
 }
 
-// stage work list of a view: every (j,k) column of every block, cut into chunks of ic planes;
-// plus the constant-mass-flux partial slots, one per (column, interior plane) of each
-// block, which do not depend on ic
+// resident stage-kernel CTAs of the whole GPU
+int stage_slots(const StageOpts& opts) {
+    int sms = 148, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int occ = stage_ctas_per_sm(opts);
+    return sms * (occ < 1 ? 1 : occ);
+}
+
+// wave split, for views with fewer (j,k) columns than resident CTAs and one plane count n0:
+// every column is cut at the same planes into q = slots / C equal chunks over [0, n0 - x)
+// (q full waves, all columns in lockstep, so halo reads of neighbouring columns hit L2), and
+// the last x planes of every column go to the r = slots - q C CTAs left over, each taking
+// the tail of columns m, m + r, m + 2 r, ... in turn (again in lockstep).  x balances the
+// chunk length against the tail CTAs' segments; each segment costs `prologue` planes more.
+// Returns the slowest CTA's cost in planes (1e300 when the split does not apply).
+double build_waves(View* v, int tj, int tk, int slots, double prologue) {
+    struct Col { int b, j0, k0; };
+    std::vector<Col> cols;
+    const int n0 = v->hb[0].n[0];
+    for (int b = 0; b < v->nblocks; ++b) {
+        const BlockDev& B = v->hb[b];
+        if (B.n[0] != n0) return 1e300;
+        for (int j0 = B.ng; j0 < B.ng + B.n[1]; j0 += tj)
+            for (int k0 = B.ng; k0 < B.ng + B.n[2]; k0 += tk) cols.push_back(Col{b, j0, k0});
+    }
+    const int C = (int)cols.size();
+    const int q = slots / C, r = slots - q * C;
+    if (q < 1 || r < 1) return 1e300;
+    const int m = (C + r - 1) / r;                 // tail segments of the busiest tail CTA
+    double best = 1e300;
+    int bx = 0;
+    for (int x = 16; x < n0 / 2; ++x) {           // tail segments of at least 16 planes
+        const double main_cost = std::ceil(double(n0 - x) / q) + prologue;
+        const double tail_cost = m * (x + prologue);
+        const double cost = std::max(main_cost, tail_cost);
+        if (cost < best - 1e-9) { best = cost; bx = x; }
+    }
+    if (bx == 0) return 1e300;
+    const int L = (n0 - bx + q - 1) / q;
+    v->tiles.clear();
+    v->cta_first.assign(1, 0);
+    for (int w = 0; w < q; ++w)
+        for (const Col& c : cols) {
+            const int ng = v->hb[c.b].ng;
+            const int lo = w * L, hi = std::min((w + 1) * L, n0 - bx);
+            if (hi > lo) v->tiles.push_back(Tile{c.b, c.j0, c.k0, ng + lo, ng + hi});
+            v->cta_first.push_back((int)v->tiles.size());
+        }
+    for (int t = 0; t < r; ++t) {
+        for (int c = t; c < C; c += r) {
+            const int ng = v->hb[cols[c].b].ng;
+            v->tiles.push_back(Tile{cols[c].b, cols[c].j0, cols[c].k0, ng + n0 - bx, ng + n0});
+        }
+        v->cta_first.push_back((int)v->tiles.size());
+    }
+    return best;
+}
+
+// constant-mass-flux partial slots of a view: one per (column, interior plane) of each block,
+// independent of how the columns are cut into CTAs
+void cmf_slots(View* v, int tj, int tk) {
+    v->cmf_slot_start.assign(1, 0);
+    for (int b = 0; b < v->nblocks; ++b) {
+        const BlockDev& B = v->hb[b];
+        const int cols = ((B.n[1] + tj - 1) / tj) * ((B.n[2] + tk - 1) / tk);
+        v->cmf_slot_start.push_back(v->cmf_slot_start.back() + cols * B.n[0]);
+    }
+    v->case_slot_start.clear();
+    for (int c = 0; c <= v->ncases; ++c) v->case_slot_start.push_back(v->cmf_slot_start[v->case_block_start[c]]);
+}
+
+// chunked split: every column cut into chunks of ic planes, one chunk per CTA
 void build_tiles(View* v, int tj, int tk, int ic) {
     v->tiles.clear();
-    v->cmf_slot_start.assign(1, 0);
+    v->cta_first.clear();
     for (int b = 0; b < v->nblocks; ++b) {
         const BlockDev& B = v->hb[b];
         const int ng = B.ng;
@@ -329,11 +402,7 @@ void build_tiles(View* v, int tj, int tk, int ic) {
             for (int j0 = ng; j0 < ng + B.n[1]; j0 += tj)
                 for (int k0 = ng; k0 < ng + B.n[2]; k0 += tk)
                     v->tiles.push_back(Tile{b, j0, k0, i0, std::min(i0 + ic, ng + B.n[0])});
-        const int cols = ((B.n[1] + tj - 1) / tj) * ((B.n[2] + tk - 1) / tk);
-        v->cmf_slot_start.push_back(v->cmf_slot_start.back() + cols * B.n[0]);
     }
-    v->case_slot_start.clear();
-    for (int c = 0; c <= v->ncases; ++c) v->case_slot_start.push_back(v->cmf_slot_start[v->case_block_start[c]]);
 }
 
 bool same_opts(const StageOpts& a, const StageOpts& b) {
@@ -396,7 +465,24 @@ int build_view(View* v, wm_case* const* cases, int n) {
         if (cases[ci]->chunk_req != req) req = 0;
     int tj, tk;
     tile_shape(v->opts.tile, &tj, &tk);
-    build_tiles(v, tj, tk, choose_chunk(v->hb, v->opts, tj, tk, req));
+    const int ic = choose_chunk(v->hb, v->opts, tj, tk, req);
+    build_tiles(v, tj, tk, ic);
+    if (req == 0) {
+        // automatic: the wave split when its slowest CTA costs less than the chunked grid's
+        // waves
+        const int slots = stage_slots(v->opts);
+        const long long nt = (long long)v->tiles.size();
+        // a segment's prologue (four planes staged and converted, two gradient planes, one
+        // face plane, with little overlap) charged as 6 planes in this comparison
+        const double chunked = double((nt + slots - 1) / slots) * (ic + 6);
+        View trial;
+        trial.hb = v->hb; trial.nblocks = v->nblocks;
+        if (build_waves(&trial, tj, tk, slots, 6.0) < chunked) {
+            v->tiles = trial.tiles;
+            v->cta_first = trial.cta_first;
+        }
+    }
+    cmf_slots(v, tj, tk);
     v->cta_start.assign(1, 0);                  // one interior cell per thread of the CFL pass
     v->gcta_start.assign(1, 0);                 // one ghost cell per thread
     for (const BlockDev& B : v->hb) {
@@ -409,6 +495,8 @@ int build_view(View* v, wm_case* const* cases, int n) {
     if ((r = m.upload(&v->d_cases, v->hc.data(), v->hc.size()))) return r;
     if ((r = m.upload(&v->d_walls, v->hw.data(), v->hw.size()))) return r;
     if ((r = m.upload(&v->d_tiles, v->tiles.data(), v->tiles.size()))) return r;
+    if (!v->cta_first.empty())
+        if ((r = m.upload(&v->d_cta_first, v->cta_first.data(), v->cta_first.size()))) return r;
     if ((r = m.upload(&v->d_case_slot_start, v->case_slot_start.data(), v->case_slot_start.size()))) return r;
     if ((r = m.upload(&v->d_seg_rhs, v->seg_rhs.data(), v->seg_rhs.size()))) return r;
     if ((r = m.upload(&v->d_seg_all, v->seg_all.data(), v->seg_all.size()))) return r;
@@ -477,6 +565,8 @@ int run_stage(View* v, Prof* pf, int stage, double* const* q_in, const double* c
     StageArgs A{};
     A.blocks = v->d_blocks; A.cases = v->d_cases; A.walls = v->d_walls;
     A.tiles = v->d_tiles; A.ntiles = (int)v->tiles.size();
+    A.cta_first = v->cta_first.empty() ? nullptr : v->d_cta_first;
+    A.nctas = v->cta_first.empty() ? A.ntiles : (int)v->cta_first.size() - 1;
     A.stage = stage;
     A.ncases = v->ncases;
     A.case_slot_start = v->d_case_slot_start;

@@ -63,7 +63,8 @@ __device__ __forceinline__ void kg_flux(const R* a, const R* b, int s, R Sx, R S
     F[4] = m * ea + p * un;
 }
 
-// KEP order 2 / 4, wmles/schemes.py:57-70
+// KEP order 2 / 4, wmles/schemes.py:57-70: 2 [(2/3) F(L,R) - (1/12) (F(L,R2) + F(L2,R))],
+// written (4/3) F(L,R) - (1/6) (...) (the outer factor 2 moved into the constants: exact)
 template <typename R>
 __device__ __forceinline__ void kep_flux(int order, const R* L2, const R* L, const R* Rr, const R* R2,
                                          int s, R Sx, R Sy, R Sz, R F[5]) {
@@ -74,7 +75,7 @@ __device__ __forceinline__ void kep_flux(int order, const R* L2, const R* L, con
         kg_flux(L2, Rr, s, Sx, Sy, Sz, Fb);
 #pragma unroll
         for (int v = 0; v < 5; ++v)
-            F[v] = R(2) * (R(2.0 / 3.0) * F[v] - R(1.0 / 12.0) * (Fa[v] + Fb[v]));
+            F[v] = R(4.0 / 3.0) * F[v] - R(1.0 / 6.0) * (Fa[v] + Fb[v]);
     }
 }
 

@@ -81,7 +81,8 @@ struct StageLayout {
     static_assert(NTH / 32 <= STAGE_MAX_WARPS, "the reduction scratch holds two sums per warp");
 };
 
-// gradient record: g[0..11] = d(u,v,w,T)/d(x,y,z), 12 = mu_eff, 13 = k_eff, 14 = theta
+// gradient record: g[0..11] = d(u,v,w,T)/d(x,y,z), 12 = mu_eff, 13 = k_eff (all at half
+// scale), 14 = theta
 enum { GS_MU = 12, GS_K = 13, GS_TH = 14 };
 
 // metric component arrays in the compute precision
@@ -100,8 +101,10 @@ __device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefe
 __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p)); }
 
 // viscous flux through one face (times area), wmles/viscous.py:28-51.  gL/gR index a
-// gradient record; pl/pr point at primitive records with component stride s; (e0, e1, e2)
-// is the unit vector from the L to the R cell centre and idist the inverse distance.
+// gradient record (half scale: the face average of two records is their sum, the same
+// value bit for bit as 0.5 (a + b), since scaling by two is exact); pl/pr point at primitive
+// records with component stride s; (e0, e1, e2) is the unit vector from the L to the R cell
+// centre and idist the inverse distance.
 template <typename R, class GL, class GR>
 __device__ __forceinline__ void viscous_flux(const R* pl, const R* pr, int s, GL gL, GR gR, R Sx, R Sy, R Sz,
                                              R e0, R e1, R e2, R idist, R F[5]) {
@@ -109,17 +112,17 @@ __device__ __forceinline__ void viscous_flux(const R* pl, const R* pr, int s, GL
     const int pv[4] = {PR_U, PR_V, PR_W, PR_T};
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
-        const R b0 = R(0.5) * (gL(3 * a) + gR(3 * a));
-        const R b1 = R(0.5) * (gL(3 * a + 1) + gR(3 * a + 1));
-        const R b2 = R(0.5) * (gL(3 * a + 2) + gR(3 * a + 2));
+        const R b0 = gL(3 * a) + gR(3 * a);
+        const R b1 = gL(3 * a + 1) + gR(3 * a + 1);
+        const R b2 = gL(3 * a + 2) + gR(3 * a + 2);
         const R corr = (pr[pv[a] * s] - pl[pv[a] * s]) * idist - (b0 * e0 + b1 * e1 + b2 * e2);
         gf[3 * a] = b0 + corr * e0;
         gf[3 * a + 1] = b1 + corr * e1;
         gf[3 * a + 2] = b2 + corr * e2;
     }
     const R div = gf[0] + gf[4] + gf[8];
-    const R muf = R(0.5) * (gL(GS_MU) + gR(GS_MU));
-    const R kf = R(0.5) * (gL(GS_K) + gR(GS_K));
+    const R muf = gL(GS_MU) + gR(GS_MU);
+    const R kf = gL(GS_K) + gR(GS_K);
     const R d23 = R(2.0 / 3.0) * div;
     const R t00 = muf * (gf[0] + gf[0] - d23), t11 = muf * (gf[4] + gf[4] - d23), t22 = muf * (gf[8] + gf[8] - d23);
     const R t01 = muf * (gf[1] + gf[3]), t02 = muf * (gf[2] + gf[6]), t12 = muf * (gf[5] + gf[7]);
@@ -159,12 +162,12 @@ __device__ __forceinline__ void face_flux(const StageOpts& o, const Phys<R>& P, 
     viscous_flux<R>(L, Rr, s, gL, gR, Sx, Sy, Sz, e0, e1, e2, idist, F);
 }
 
+// one segment of a CTA's work: tile t (a (j,k) column of one block over planes [t.i0, t.i1))
 template <typename R, int SCHEME, int TJ, int TK>
-__global__ void __launch_bounds__(StageLayout<R, SCHEME, TJ, TK>::NTH, StageLayout<R, SCHEME, TJ, TK>::MIN_CTAS)
-    stage_kernel(const __grid_constant__ StageArgs A, const StageOpts o) {
+__device__ __forceinline__ void stage_segment(const StageArgs& A, const StageOpts& o, const Tile t,
+                                              unsigned char* smem_raw) {
     using LY = StageLayout<R, SCHEME, TJ, TK>;
     constexpr int NT = LY::NT, NTH = LY::NTH, PK = LY::PK, PN = LY::PN, GK = LY::GK, GN = LY::GN, NGS = LY::NGS;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     double* qs = reinterpret_cast<double*>(smem_raw + LY::qs_off);
     R* pr = reinterpret_cast<R*>(smem_raw + LY::pr_off);
     R* gs = reinterpret_cast<R*>(smem_raw + LY::gs_off);
@@ -172,7 +175,6 @@ __global__ void __launch_bounds__(StageLayout<R, SCHEME, TJ, TK>::NTH, StageLayo
     R* fk = reinterpret_cast<R*>(smem_raw + LY::fk_off);
     double* red = reinterpret_cast<double*>(smem_raw + LY::red_off);
 
-    const Tile t = A.tiles[blockIdx.x];
     const BlockDev B = A.blocks[t.blk];
     const CaseDev& C = A.cases[B.case_id];
     const Phys<R> P(C);
@@ -239,7 +241,10 @@ __global__ void __launch_bounds__(StageLayout<R, SCHEME, TJ, TK>::NTH, StageLayo
             const R Hjx = __ldg(mj + WM_MET_SJX * nc), Hjy = __ldg(mj + WM_MET_SJY * nc), Hjz = __ldg(mj + WM_MET_SJZ * nc);
             const R Skx = __ldg(m + WM_MET_SKX * nc), Sky = __ldg(m + WM_MET_SKY * nc), Skz = __ldg(m + WM_MET_SKZ * nc);
             const R Hkx = __ldg(mk + WM_MET_SKX * nc), Hky = __ldg(mk + WM_MET_SKY * nc), Hkz = __ldg(mk + WM_MET_SKZ * nc);
-            const R ivol = __ldg(m + WM_MET_IVOL * nc);
+            // half of 1/V: the record holds half the gradient (faces average two records by
+            // adding them); the SGS models are homogeneous of degree one in the gradient and
+            // the Ducros sensor of degree zero, so they take the half gradient directly
+            const R hivol = R(0.5) * __ldg(m + WM_MET_IVOL * nc);
             const R delta = sgs_model != WM_SGS_NONE ? __ldg(m + WM_MET_DELTA * nc) : R(0);
             R acc[12];
 #pragma unroll
@@ -253,15 +258,18 @@ __global__ void __launch_bounds__(StageLayout<R, SCHEME, TJ, TK>::NTH, StageLayo
                 acc[3 * a + 2] = ((hi * Hiz - li * Siz) + (hj * Hjz - lj * Sjz)) + (hk * Hkz - lk * Skz);
             }
 #pragma unroll
-            for (int q = 0; q < 12; ++q) acc[q] *= ivol;
+            for (int q = 0; q < 12; ++q) acc[q] *= hivol;
             const R T = P0[PR_T * PN + pc];
-            const R mu = sutherland(T, P);
-            R mut = R(0);
-            if (sgs_model != WM_SGS_NONE) mut = P0[PR_RHO * PN + pc] * sgs_nut(sgs_model, acc, delta, P.sgs_c);
+            const R muh = R(0.5) * sutherland(T, P);              // half the molecular viscosity
+            R muth = R(0);                                        // half the eddy viscosity
+            if (sgs_model != WM_SGS_NONE) {
+                const R rho = P0[PR_RHO * PN + pc];
+                muth = rho * sgs_nut(sgs_model, acc, delta, P.sgs_c);
+            }
 #pragma unroll
             for (int q = 0; q < 12; ++q) gs[q * GN + c] = acc[q];
-            gs[GS_MU * GN + c] = mu + mut;
-            gs[GS_K * GN + c] = P.cp * (mu * P.inv_Pr + mut * P.inv_Prt);
+            gs[GS_MU * GN + c] = muh + muth;
+            gs[GS_K * GN + c] = P.cp * (muh * P.inv_Pr + muth * P.inv_Prt);
             if constexpr (NGS > 14) gs[GS_TH * GN + c] = ducros(acc);
         }
     };
@@ -521,14 +529,33 @@ __global__ void __launch_bounds__(StageLayout<R, SCHEME, TJ, TK>::NTH, StageLayo
         }
     }
 
+}
+
+template <typename R, int SCHEME, int TJ, int TK>
+__global__ void __launch_bounds__(StageLayout<R, SCHEME, TJ, TK>::NTH, StageLayout<R, SCHEME, TJ, TK>::MIN_CTAS)
+    stage_kernel(const __grid_constant__ StageArgs A, const StageOpts o) {
+    using LY = StageLayout<R, SCHEME, TJ, TK>;
+    constexpr int NTH = LY::NTH;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* red = reinterpret_cast<double*>(smem_raw + LY::red_off);
+    const int tid = threadIdx.x;
+    // this CTA's segments: one tile, or a balanced range of tiles (consecutive column pieces)
+    const int first = A.cta_first ? A.cta_first[blockIdx.x] : blockIdx.x;
+    const int last = A.cta_first ? A.cta_first[blockIdx.x + 1] : blockIdx.x + 1;
+#pragma unroll 1
+    for (int ti = first; ti < last; ++ti) {
+        stage_segment<R, SCHEME, TJ, TK>(A, o, A.tiles[ti], smem_raw);
+        __syncthreads();                 // shared memory is reused by the next segment
+    }
+
     if (A.stage == 3 && A.cmf_part != nullptr) {
         // every CTA of the launch signals; the last one reduces each case's partials
-        __shared__ bool last;
-        if (cmf_on && tid == 0) __threadfence();
+        __shared__ bool last_cta;
+        if (tid == 0) __threadfence();
         __syncthreads();
-        if (tid == 0) last = atomicAdd(A.cmf_counter, 1u) == unsigned(gridDim.x - 1);
+        if (tid == 0) last_cta = atomicAdd(A.cmf_counter, 1u) == unsigned(gridDim.x - 1);
         __syncthreads();
-        if (last) {
+        if (last_cta) {
             // per case: the sum over that case's partials in slot order (the same alone or in
             // a batch, for any chunk length, run to run) and the shift
             // delta = target - sum(rho u V) / sum(V), wmles/solver.py:24-29
@@ -574,7 +601,7 @@ static cudaError_t launch_one(const StageArgs& A, const StageOpts& o, cudaStream
     using LY = StageLayout<R, SCHEME, TJ, TK>;
     cudaError_t e = configure_one<R, SCHEME, TJ, TK>();
     if (e != cudaSuccess) return e;
-    stage_kernel<R, SCHEME, TJ, TK><<<A.ntiles, LY::NTH, LY::bytes, s>>>(A, o);
+    stage_kernel<R, SCHEME, TJ, TK><<<A.nctas, LY::NTH, LY::bytes, s>>>(A, o);
     return cudaGetLastError();
 }
 

@@ -86,6 +86,8 @@ struct StageArgs {
     const WallDev* walls;
     const Tile* tiles;
     int ntiles;
+    const int* cta_first;         // CTA c runs tiles [cta_first[c], cta_first[c+1]); null: tile c
+    int nctas;                    // grid size
     int stage;                    // 0: q_out = RHS; 1,2,3: SSP-RK3 stage
     int ncases;
     const int* case_slot_start;   // ncases + 1: partial-sum slots of case c are [start[c], start[c+1])
