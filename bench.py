@@ -42,10 +42,15 @@ N_CFG2 = (256, 128, 128)
 # stages, from one ncu capture of the same kernel on a 128^3 case of this workload; scaled
 # by the cell count for the roofline's `traffic`
 TRAFFIC_PER_CELL = {"fp64": 321.0, "mixed": 229.0}
-# FP64 floating-point operations per interior cell per stage-kernel launch (FP64 form), from
-# the same kind of capture (None until measured for the current kernel)
-FP64_FLOP_PER_CELL = None
-FP64_PEAK_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
+# FP64 work per interior cell per stage-kernel launch (FP64 form, mean of the three RK
+# stages), from one ncu capture of the same kernel on a 128^3 case of this workload: DADD 285.6,
+# DMUL 366.5, DFMA 365.3 thread instructions, i.e. 1383 flop (an FMA counts two) in 1017
+# FP64-pipe instructions
+FP64_FLOP_PER_CELL = 1383.0
+FP64_INST_PER_CELL = 1017.0
+# nominal FP64 rate of a B200: 148 SMs x 64 FP64 lanes x 1.965 GHz (x 2 flop per FMA)
+FP64_PEAK_INST = 148 * 64 * 1.965e9
+FP64_PEAK_TFLOPS = 2 * FP64_PEAK_INST / 1e12
 
 
 def peaks():
@@ -331,12 +336,15 @@ def run_ours(args, rank, world, local_rank):
         # the FP64 stage kernel's other roof: its FP64 instructions against the FP64 pipe
         fl = FP64_FLOP_PER_CELL * cells
         tfs = fl / (f["stage_ms"] * 1e-3) / 1e12
+        inst_rate = FP64_INST_PER_CELL * cells / (f["stage_ms"] * 1e-3)
         line["roofline"]["fp64_pipe"] = {
             "achieved": tfs, "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s", "frac": tfs / FP64_PEAK_TFLOPS,
             "flop_per_launch": fl, "flop_per_cell": FP64_FLOP_PER_CELL,
+            "pipe_inst_per_cell": FP64_INST_PER_CELL, "pipe_frac": inst_rate / FP64_PEAK_INST,
             "flop_source": "ncu: 2 x dfma + dadd + dmul thread instructions per launch (mean of the three "
                            "RK stages) on a 128^3 case of the workload, per interior cell",
-            "peak_source": "nominal: 148 SMs x 64 FP64 FMA per clock x 2 x 1.965 GHz"}
+            "peak_source": "nominal: 148 SMs x 64 FP64 lanes x 1.965 GHz (x 2 flop per FMA); pipe_frac "
+                           "counts FP64 instructions against the lanes (DADD and DMUL take a lane like DFMA)"}
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.cpu_cells)
     if world == 1 and args.extra:
