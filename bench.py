@@ -41,7 +41,7 @@ N_CFG2 = (256, 128, 128)
 # DRAM bytes (read + write) per stage-kernel launch per interior cell, mean of the three RK
 # stages, from one ncu capture of the same kernel on a 128^3 case of this workload; scaled
 # by the cell count for the roofline's `traffic`
-TRAFFIC_PER_CELL = {"fp64": 321.0, "mixed": 229.0}
+TRAFFIC_PER_CELL = {"fp64": 325.0, "mixed": 229.0}
 # FP64 work per interior cell per stage-kernel launch (FP64 form, mean of the three RK
 # stages), from one ncu capture of the same kernel on a 128^3 case of this workload: DADD 285.6,
 # DMUL 366.5, DFMA 365.3 thread instructions, i.e. 1383 flop (an FMA counts two) in 1017

@@ -2,19 +2,23 @@
 //
 // One CTA owns a TJ x TK tile of (j,k) columns of one block and marches along i over a
 // chunk of planes [i0, i1).  Shared memory holds
-//   pr[4]  primitive records of planes i-2..i+1 on the tile + 2-cell halo (rolling ring)
-//   qs     the conservative values of plane i+2 on the same footprint, arriving by
-//          cp.async while plane i is being computed
+//   pr[5]  primitive records of planes i-2..i+2 on the tile + 2-cell halo (rolling ring;
+//          four slots, planes i-2..i+1, in the float form and the tiles that run several
+//          CTAs per SM)
+//   qs     the conservative values of the next plane to convert on the same footprint,
+//          arriving by cp.async while plane i is being computed
 //   gs     Green-Gauss gradients, mu_eff, k_eff (and the Ducros sensor) of plane i on the
 //          tile + 1-cell halo
 //   fj/fk  the j- and k-face fluxes of plane i
 // and registers, per column, the previous i-face flux, the j/k flux differences of the
-// previous plane and that plane's gradient record.  Per plane there are three phases
+// previous plane and that plane's gradient record.  Per plane there are two phases
 // separated by barriers:
-//   1. primitives of plane i+1 from the staged conservative values
-//   2. gradient records of plane i
-//   3. own i-face flux -> RK epilogue of plane i-1; all j/k faces of plane i (flat loop);
-//      the cp.async of plane i+2 is in flight meanwhile
+//   1. gradient records of plane i; the warps without a record convert the staged plane
+//      i+2 to primitives
+//   2. own i-face flux -> RK epilogue of plane i-1; all j/k faces of plane i (flat loop);
+//      the cp.async of plane i+3 is in flight meanwhile
+// (float form, or several CTAs per SM: three phases, the conversion of plane i+1 first and
+// on its own).
 // Each face flux is evaluated once; each conservative value is read from HBM about once
 // per stage (halo re-reads hit L2).  Stage 3 also emits per-(column, plane) partial sums of
 // rho u V for the constant-mass-flux constraint.
@@ -67,18 +71,30 @@ struct StageLayout {
     static constexpr int GJ = TJ + 2, GK = TK + 2, GN = GJ * GK;   // gradients: 1-cell halo
     static constexpr int NGS = (SCHEME == WM_SCHEME_HYBRID) ? 15 : 14;
     static constexpr int FJN = (TJ + 1) * TK, FKN = TJ * (TK + 1);
-    static constexpr size_t qs_off = 0;                                        // double [5][PN]
-    static constexpr size_t pr_off = qs_off + sizeof(double) * 5 * PN;         // R [4][PR_N][PN]
-    static constexpr size_t gs_off = pr_off + sizeof(R) * 4 * PR_N * PN;       // R [NGS][GN]
-    static constexpr size_t fj_off = gs_off + sizeof(R) * NGS * GN;            // R [5][FJN]
-    static constexpr size_t fk_off = fj_off + sizeof(R) * 5 * FJN;             // R [5][FKN]
-    static constexpr size_t red_off = (fk_off + sizeof(R) * 5 * FKN + 15) / 16 * 16;
-    static constexpr size_t bytes = red_off + sizeof(double) * 2 * STAGE_MAX_WARPS;
     // resident CTAs per SM the register budget is sized for: the FP64 form of the 256-thread
     // tiles needs ~250 registers and 170+ KB of shared memory (one CTA); the float form
     // fits two 256-thread CTAs (<= 128 registers, ~96 KB each) or three 128-thread CTAs
     static constexpr int MIN_CTAS = stage_min_ctas(sizeof(R), NTH);
+    // FP64, one CTA per SM: a fifth primitive slot (the shared memory is there), so plane
+    // i+2 is converted while the gradient records of plane i are computed, by the warps that
+    // have no record to compute, and a plane takes two barriers instead of three.  FP64 stage
+    // time per step, channel 256x128x128 / smooth ramp 384x96x64 / NACA C-grid (configs 2 / 3 /
+    // 4): 2.62 / 2.63 / 2.91 ms against 2.70 / 2.75 / 2.93 with three phases.  The float
+    // form's one-CTA 16 x 32 tile has a record for nearly every thread (612 records, 640
+    // threads) and gains nothing (ramp / C-grid 1.17 / 1.09 ms against 1.17 / 1.08): it keeps
+    // three phases.
+    static constexpr bool FUSE = MIN_CTAS == 1 && sizeof(R) == 8;
+    static constexpr int NSLOT = FUSE ? 5 : 4;
+    static constexpr size_t qs_off = 0;                                        // double [5][PN]
+    static constexpr size_t pr_off = qs_off + sizeof(double) * 5 * PN;         // R [NSLOT][PR_N][PN]
+    static constexpr size_t gs_off = pr_off + sizeof(R) * NSLOT * PR_N * PN;   // R [NGS][GN]
+    static constexpr size_t fj_off = gs_off + sizeof(R) * NGS * GN;            // R [5][FJN]
+    static constexpr size_t fk_off = fj_off + sizeof(R) * 5 * FJN;             // R [5][FKN]
+    static constexpr size_t red_off = (fk_off + sizeof(R) * 5 * FKN + 15) / 16 * 16;
+    static constexpr size_t bytes = red_off + sizeof(double) * 2 * STAGE_MAX_WARPS;
     static_assert(NTH / 32 <= STAGE_MAX_WARPS, "the reduction scratch holds two sums per warp");
+    static_assert(!FUSE || GN <= NTH, "the fused phase computes one gradient record per thread");
+    static_assert(bytes <= 227 * 1024, "shared memory of one CTA");
 };
 
 // gradient record: g[0..11] = d(u,v,w,T)/d(x,y,z), 12 = mu_eff, 13 = k_eff (all at half
@@ -206,26 +222,29 @@ __device__ __forceinline__ void stage_segment(const StageArgs& A, const StageOpt
             for (int v = 0; v < 5; ++v) cp_async8(qs + v * PN + c, SP.q_in + v * nc + idx);
         }
     };
-    // ---- staged values -> primitive records in ring slot
-    auto convert_plane = [&](int slot) {
-        R* dst = pr + slot * PR_N * PN;
-        for (int c = tid; c < PN; c += NTH) {
-            double q[5];
+    // ring slot of plane ip's primitive records
+    auto slot = [](int ip) { return LY::FUSE ? ip % LY::NSLOT : ip & 3; };
+    // ---- staged value c -> primitive record c of plane ip
+    auto convert_cell = [&](int ip, int c) {
+        R* dst = pr + slot(ip) * PR_N * PN;
+        double q[5];
 #pragma unroll
-            for (int v = 0; v < 5; ++v) q[v] = qs[v * PN + c];
-            R rec[PR_N];
-            cons_to_rec(q, P, rec);
+        for (int v = 0; v < 5; ++v) q[v] = qs[v * PN + c];
+        R rec[PR_N];
+        cons_to_rec(q, P, rec);
 #pragma unroll
-            for (int v = 0; v < PR_N; ++v) dst[v * PN + c] = rec[v];
-        }
+        for (int v = 0; v < PR_N; ++v) dst[v * PN + c] = rec[v];
+    };
+    auto convert_plane = [&](int ip) {
+        for (int c = tid; c < PN; c += NTH) convert_cell(ip, c);
     };
 
-    // ---- gradient records of plane ip (ring slots of ip-1, ip, ip+1) on the tile + 1-cell halo
-    auto grad_plane = [&](int ip) {
-        const R* Pm = pr + ((ip - 1) & 3) * PR_N * PN;
-        const R* P0 = pr + (ip & 3) * PR_N * PN;
-        const R* Pp = pr + ((ip + 1) & 3) * PR_N * PN;
-        for (int c = tid; c < GN; c += NTH) {
+    // ---- gradient record c of plane ip (ring slots of ip-1, ip, ip+1) on the tile + 1-cell halo
+    auto grad_cell = [&](int ip, int c) {
+        const R* Pm = pr + slot(ip - 1) * PR_N * PN;
+        const R* P0 = pr + slot(ip) * PR_N * PN;
+        const R* Pp = pr + slot(ip + 1) * PR_N * PN;
+        {
             const int jj = c / GK, kk = c - jj * GK;
             const int pc = (jj + 1) * PK + (kk + 1);
             const int gj = min(t.j0 - 1 + jj, Nj - 2), gk = min(t.k0 - 1 + kk, Nk - 2);
@@ -273,6 +292,29 @@ __device__ __forceinline__ void stage_segment(const StageArgs& A, const StageOpt
             if constexpr (NGS > 14) gs[GS_TH * GN + c] = ducros(acc);
         }
     };
+    auto grad_plane = [&](int ip) {
+        for (int c = tid; c < GN; c += NTH) grad_cell(ip, c);
+    };
+    // ---- gradient records of plane ip and (conv) primitives of plane ip+2 from the staging
+    // buffer.  The warps that hold a record take one each; the warps left over convert (at
+    // most five cells each, about the time of one record), and the cells beyond their share
+    // go to the record warps after their record.  (The 8 x 32 and 16 x 16 KEP tiles: 96
+    // converting threads, every cell theirs.  Three or four rounds for the converting warps,
+    // the rest on the record warps: 1.1-1.4 % slower on the channel, the same on the ramp and
+    // the C-grid.)
+    auto grad_convert = [&](int ip, bool conv) {
+        constexpr int GW = (GN + 31) / 32 * 32;          // threads of the record warps
+        constexpr int SP = NTH - GW;                     // threads of the converting warps
+        constexpr int CR = SP > 0 ? (PN + SP - 1) / SP < 5 ? (PN + SP - 1) / SP : 5 : 0;
+        constexpr int CS = SP * CR;                      // cells the converting warps take
+        if (tid < GW) {
+            if (tid < GN) grad_cell(ip, tid);
+            if (conv)
+                for (int c = CS + tid; c < PN; c += GW) convert_cell(ip + 2, c);
+        } else if (conv) {
+            for (int c = tid - GW; c < CS && c < PN; c += SP) convert_cell(ip + 2, c);
+        }
+    };
 
     // wall-model flux override of face (axis, side) at tangential position (a, b)
     auto wall_flux = [&](int face, int a, int b, R F[5]) -> bool {
@@ -295,10 +337,10 @@ __device__ __forceinline__ void stage_segment(const StageArgs& A, const StageOpt
         if (ip == ihi && wall_flux(1, j, k, F)) return;
         const int pc = (tj + 2) * PK + (tk + 2);
         const int gc = (tj + 1) * GK + (tk + 1);
-        const R* L2 = pr + ((ip - 2) & 3) * PR_N * PN + pc;
-        const R* L = pr + ((ip - 1) & 3) * PR_N * PN + pc;
-        const R* Rr = pr + (ip & 3) * PR_N * PN + pc;
-        const R* R2 = pr + ((ip + 1) & 3) * PR_N * PN + pc;
+        const R* L2 = pr + slot(ip - 2) * PR_N * PN + pc;
+        const R* L = pr + slot(ip - 1) * PR_N * PN + pc;
+        const R* Rr = pr + slot(ip) * PR_N * PN + pc;
+        const R* R2 = pr + slot(ip + 1) * PR_N * PN + pc;
         const R* m = MB + (ip * planei + j * Nk + k);
         const R Sx = __ldg(m + WM_MET_SIX * nc), Sy = __ldg(m + WM_MET_SIY * nc), Sz = __ldg(m + WM_MET_SIZ * nc);
         const R e0 = __ldg(m + WM_MET_EIX * nc), e1 = __ldg(m + WM_MET_EIY * nc), e2 = __ldg(m + WM_MET_EIZ * nc);
@@ -309,7 +351,7 @@ __device__ __forceinline__ void stage_segment(const StageArgs& A, const StageOpt
 
     // ---- one j- (f < FJN) or k-face flux of plane ip into shared memory
     auto jk_face = [&](int ip, int f) {
-        const R* P0 = pr + (ip & 3) * PR_N * PN;
+        const R* P0 = pr + slot(ip) * PR_N * PN;
         R F[5] = {R(0), R(0), R(0), R(0), R(0)};
         if (f < LY::FJN) {
             const int row = f / TK, kk = f - row * TK;
@@ -468,16 +510,18 @@ __device__ __forceinline__ void stage_segment(const StageArgs& A, const StageOpt
         }
     };
 
-    // ---- prologue: planes i0-2 .. i0+1, gradients of i0-1 and i0, faces of plane i0
+    // ---- prologue: planes i0-2 .. i0+1 (and i0+2 when fused), gradients of i0-1 and i0,
+    // faces of plane i0
+    constexpr int PRE = LY::FUSE ? 2 : 1;          // last plane converted ahead of the march
 #pragma unroll 1
-    for (int ip = i0 - 2; ip <= i0 + 1; ++ip) {
+    for (int ip = i0 - 2; ip <= i0 + PRE; ++ip) {
         stage_plane(ip);
         cp_async_wait_all();
         __syncthreads();
-        convert_plane(ip & 3);
+        convert_plane(ip);
         __syncthreads();
     }
-    stage_plane(i0 + 2);                 // in flight during the prologue's compute
+    if (i0 + PRE + 1 <= i1 + 1) stage_plane(i0 + PRE + 1);   // in flight during the prologue's compute
     grad_plane(i0 - 1);
     __syncthreads();
     save_gs();
@@ -485,20 +529,27 @@ __device__ __forceinline__ void stage_segment(const StageArgs& A, const StageOpt
     grad_plane(i0);
     __syncthreads();
     if (active) iface_flux(i0, Flo);
+    if constexpr (LY::FUSE) save_gs();   // before the barrier: no barrier precedes the next records
     for (int f = rtid; f < LY::FJN + LY::FKN; f += NTH) jk_face(i0, f);
     cp_async_wait_all();
     __syncthreads();
     jk_diff();
-    save_gs();
+    if constexpr (!LY::FUSE) save_gs();
 
     // ---- march: iteration ip outputs plane ip-1
 #pragma unroll 1
     for (int ip = i0 + 1; ip <= i1; ++ip) {
-        convert_plane((ip + 1) & 3);     // staged plane ip+1 -> primitives
-        __syncthreads();
-        grad_plane(ip);
-        __syncthreads();
-        if (ip + 2 <= i1 + 1) stage_plane(ip + 2);
+        if constexpr (LY::FUSE) {
+            grad_convert(ip, ip < i1);   // records of plane ip; staged plane ip+2 -> primitives
+            __syncthreads();
+            if (ip + 3 <= i1 + 1) stage_plane(ip + 3);
+        } else {
+            convert_plane(ip + 1);       // staged plane ip+1 -> primitives
+            __syncthreads();
+            grad_plane(ip);
+            __syncthreads();
+            if (ip + 2 <= i1 + 1) stage_plane(ip + 2);
+        }
         if (ip < i1) prefetch_next(ip);
         if (active) {
             R Fhi[5];
@@ -507,6 +558,7 @@ __device__ __forceinline__ void stage_segment(const StageArgs& A, const StageOpt
 #pragma unroll
             for (int v = 0; v < 5; ++v) Flo[v] = Fhi[v];
         }
+        if constexpr (LY::FUSE) save_gs();
         if (cmf_on) {
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) cmf_acc += __shfl_down_sync(0xffffffffu, cmf_acc, off);
@@ -525,7 +577,7 @@ __device__ __forceinline__ void stage_segment(const StageArgs& A, const StageOpt
         }
         if (ip < i1) {
             jk_diff();
-            save_gs();
+            if constexpr (!LY::FUSE) save_gs();
         }
     }
 
