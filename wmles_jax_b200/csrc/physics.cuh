@@ -230,7 +230,7 @@ __device__ __forceinline__ double spalding_utau(double kappa, double ekb, int n_
                                                 double rho_w, double mu_w, bool* moving) {
     const double Reh = h * U * rho_w / mu_w;
     double up = fmin(fmax(sqrt(Reh), 1.0), 25.0);
-    double last = 0.0;
+    double last = 0.0, prev = up;
     *moving = false;
     for (int it = 0; it < n_iter; ++it) {
         const double ku = kappa * up;
@@ -241,7 +241,17 @@ __device__ __forceinline__ double spalding_utau(double kappa, double ekb, int n_
         // the update is a fixed function of up: once an iterate repeats exactly, every later
         // one does too, so stopping here returns what all n_iter iterations would
         if (next == up) return U / up;
+        // period two (about one face in ten ends alternating between two neighbouring
+        // doubles, and one such lane kept its whole warp iterating to n_iter): the iterates
+        // from prev on are prev, up, prev, ..., so the last of n_iter is prev (= next) when
+        // n_iter - (it - 1) is even, else up
+        if (it > 0 && next == prev) {
+            const double fin = ((n_iter - it + 1) & 1) == 0 ? next : up;
+            *moving = !(fabs(next - up) <= 1e-8 * fin);
+            return U / fin;
+        }
         last = next - up;
+        prev = up;
         up = next;
     }
     *moving = !(fabs(last) <= 1e-8 * up);
