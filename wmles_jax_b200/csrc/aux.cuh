@@ -89,6 +89,8 @@ struct SpongeArgs {
     const BlockDev* blocks;
     const CaseDev* cases;
     int nblocks;
+    int nrows;                     // rows that reach into a sponge, over the view's blocks
+    const int* rows;               // nrows x (view block, interior row (i - ng) * nj + (j - ng))
     const double* q[WM_MAX_BLOCKS];
     double* mean[WM_MAX_BLOCKS];   // 5 x Ni x Nj
 };
@@ -116,7 +118,7 @@ struct SurfaceArgs {
     GhostArgs G;
     WallArgs W;
     SpongeArgs S;          // nblocks = 0: no sponge
-    int g_ctas, w_per, w_ctas, s_per, s_ctas;
+    int g_ctas, w_per, w_ctas, s_ctas;
 };
 
 __device__ __forceinline__ long long cell_index(const BlockDev& B, int axis, int c, int a, int b) {
@@ -134,11 +136,14 @@ __device__ __forceinline__ double sutherland_d(double T, const CaseDev& C) {
 }
 
 cudaError_t launch_ghost(const GhostArgs& G, cudaStream_t s);
-cudaError_t launch_surface(SurfaceArgs& A, int max_sponge_rows, cudaStream_t s);
+cudaError_t launch_surface(SurfaceArgs& A, cudaStream_t s);
 cudaError_t launch_wall(const WallArgs& W, cudaStream_t s);
 cudaError_t launch_dt(const DtArgs& D, cudaStream_t s);
 cudaError_t launch_status_gather(const CaseDev* cases, int ncases, unsigned* out, cudaStream_t s);
-cudaError_t launch_sponge_mean(const SpongeArgs& S, int max_rows, cudaStream_t s);
+// set-up: flags[row] = 1 for the interior (i, j) rows of a block with a cell inside the
+// sponge (xcx: the block's cell-centre x metric; invL, xs, inv_dx: the case's sponge constants)
+cudaError_t launch_sponge_flags(const double* xcx, long long plane, int Nk, int ng, int ni, int nj, int nk,
+                                double invL, double xs, double inv_dx, unsigned char* flags, cudaStream_t s);
 cudaError_t launch_inflow(const InflowArgs& I, int Nj, int Nk, int ng, cudaStream_t s);
 
 }  // namespace wm

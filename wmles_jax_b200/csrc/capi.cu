@@ -157,6 +157,7 @@ struct wm_case {
     wm_inflow inflow{};
     long long inflow_n = 0;
     std::vector<double*> spmean;         // per block, null without sponge
+    std::vector<int> sp_rows;            // (block, interior row) pairs of the rows that reach into the sponge
     double* ps_part = nullptr;           // plane-statistics scratch (PS_NQ x max Nj x PS_CHUNKS)
     unsigned* ps_counter = nullptr;
     View* self = nullptr;                // the case as a view of one case
@@ -193,7 +194,9 @@ struct View {
     unsigned* counters = nullptr;        // [0]: CFL reduction, [1]: constant-mass-flux reduction
     std::vector<int> cta_start;          // CFL pass: first CTA of each view block (+ total)
     std::vector<int> gcta_start;         // same for the blocks' ghost cells (output ghost fill)
-    int max_wall_faces = 0, sponge_rows = 0;
+    int max_wall_faces = 0;
+    std::vector<int> sp_rows;            // (view block, row) pairs of the sponge rows of every case
+    int* d_sp_rows = nullptr;
     bool any_sponge = false, any_cmf = false;
     StageOpts opts{};
 };
@@ -450,8 +453,10 @@ int build_view(View* v, wm_case* const* cases, int n) {
         v->total_rhs += c->prog_rhs.count;
         v->seg_all.push_back(segment(c, c->prog_all, v->total_all, bo));
         v->total_all += c->prog_all.count;
-        for (size_t b = 0; b < c->hb.size(); ++b)
-            if (c->spmean[b]) v->sponge_rows = std::max(v->sponge_rows, c->hb[b].n[0] * c->hb[b].n[1]);
+        for (size_t p = 0; p < c->sp_rows.size(); p += 2) {
+            v->sp_rows.push_back(bo + c->sp_rows[p]);
+            v->sp_rows.push_back(c->sp_rows[p + 1]);
+        }
         v->any_sponge = v->any_sponge || c->hc.sponge;
         v->any_cmf = v->any_cmf || c->hc.cmf_dir >= 0;
     }
@@ -500,6 +505,8 @@ int build_view(View* v, wm_case* const* cases, int n) {
     if ((r = m.upload(&v->d_case_slot_start, v->case_slot_start.data(), v->case_slot_start.size()))) return r;
     if ((r = m.upload(&v->d_seg_rhs, v->seg_rhs.data(), v->seg_rhs.size()))) return r;
     if ((r = m.upload(&v->d_seg_all, v->seg_all.data(), v->seg_all.size()))) return r;
+    if (!v->sp_rows.empty())
+        if ((r = m.upload(&v->d_sp_rows, v->sp_rows.data(), v->sp_rows.size()))) return r;
     if ((r = m.alloc(&v->cmf_part, (size_t)v->cmf_slot_start.back()))) return r;
     if ((r = m.alloc(&v->cmf_delta, (size_t)n))) return r;
     CK(cudaMemset(v->cmf_delta, 0, sizeof(double) * n));
@@ -549,6 +556,7 @@ int run_stage(View* v, Prof* pf, int stage, double* const* q_in, const double* c
     std::vector<const double*> spm(v->nblocks, nullptr);
     if (v->any_sponge) {
         U.S.blocks = v->d_blocks; U.S.cases = v->d_cases; U.S.nblocks = v->nblocks;
+        U.S.nrows = (int)v->sp_rows.size() / 2; U.S.rows = v->d_sp_rows;
         for (int ci = 0; ci < v->ncases; ++ci)
             for (size_t b = 0; b < v->members[ci]->hb.size(); ++b) {
                 const int vb = v->case_block_start[ci] + (int)b;
@@ -560,7 +568,7 @@ int run_stage(View* v, Prof* pf, int stage, double* const* q_in, const double* c
     {
         const bool any = U.G.total > 0 || !v->hw.empty() || v->any_sponge;
         LaunchScope ls(pf, WM_KIND_GHOST, s, any ? 1 : 0);
-        CK(launch_surface(U, v->sponge_rows, s));
+        CK(launch_surface(U, s));
     }
     StageArgs A{};
     A.blocks = v->d_blocks; A.cases = v->d_cases; A.walls = v->d_walls;
@@ -800,6 +808,15 @@ int wm_case_create(const wm_case_desc* d, wm_case** out) {
             if ((r = c->mem.alloc(&c->spmean[b], 5 * (size_t)B.N[0] * B.N[1]))) return bail(r);
             // rows outside the sponge are never written (their mean is not needed): keep them 0
             CKB(cudaMemset(c->spmean[b], 0, sizeof(double) * 5 * B.N[0] * B.N[1]));
+            const int rows = B.n[0] * B.n[1];
+            unsigned char* d_flags = nullptr;
+            if ((r = c->mem.alloc(&d_flags, (size_t)rows))) return bail(r);
+            CKB(launch_sponge_flags(B.met + (size_t)WM_MET_XCX * B.ncell, B.plane, B.N[2], B.ng, B.n[0], B.n[1],
+                                    B.n[2], C.sp_invL, C.sp_xs, C.sp_inv_dx, d_flags, 0));
+            std::vector<unsigned char> flags((size_t)rows);
+            CKB(cudaMemcpy(flags.data(), d_flags, (size_t)rows, cudaMemcpyDeviceToHost));
+            for (int row = 0; row < rows; ++row)
+                if (flags[row]) { c->sp_rows.push_back(b); c->sp_rows.push_back(row); }
         }
     }
 

@@ -247,24 +247,14 @@ cudaError_t launch_wall(const WallArgs& W, cudaStream_t s) {
 
 // ------------------------------------------------------------------ sponge
 // volume-weighted spanwise mean of q over interior k, per interior (i, j) row
-// (SmoothRampSponge.__call__, wmles/smooth_ramp.py:212-216)
-// one warp per row (row uniform across the warp: the shuffles below see all 32 lanes)
+// (SmoothRampSponge.__call__, wmles/smooth_ramp.py:212-216), for the rows listed at case
+// creation (sponge_flags_kernel); one warp per row (the shuffles below see all 32 lanes)
 __device__ __forceinline__ void sponge_row(const SpongeArgs& S, int b, int row, int lane) {
-    if (S.mean[b] == nullptr) return;    // block of a case without a sponge
     const BlockDev& B = S.blocks[b];
-    const int ng = B.ng, ni = B.n[0], nj = B.n[1], nk = B.n[2];
-    if (row >= ni * nj) return;
+    const int ng = B.ng, nj = B.n[1], nk = B.n[2];
     const int i = row / nj + ng, j = row % nj + ng;
     const long long N = B.ncell;
     const long long base = i * B.plane + (long long)j * B.N[2];
-    // a row whose every cell lies before the sponge start needs no mean: the stage kernel's
-    // sponge term there is sigma * (q - mean) with sigma exactly 0 (the same expression as its
-    // ramp argument decides it), and the row's mean stays at its initial 0
-    const CaseDev& C = S.cases[B.case_id];
-    bool active = false;
-    for (int k = ng + lane; k < ng + nk; k += 32)
-        active |= (B.met[WM_MET_XCX * N + base + k] * C.sp_invL - C.sp_xs) * C.sp_inv_dx > 0.0;
-    if (!__any_sync(0xffffffffu, active)) return;
     const double* q = S.q[b];
     double acc[5] = {0, 0, 0, 0, 0}, vs = 0.0;
     for (int k = ng + lane; k < ng + nk; k += 32) {
@@ -287,13 +277,27 @@ __device__ __forceinline__ void sponge_row(const SpongeArgs& S, int b, int row, 
     }
 }
 
-__global__ void sponge_mean_kernel(const __grid_constant__ SpongeArgs S) {
-    sponge_row(S, blockIdx.y, blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5), threadIdx.x & 31);
+// A row whose every cell lies before the sponge start needs no mean: the stage kernel's
+// sponge term there is sigma * (q - mean) with sigma exactly 0 (the same expression as its
+// ramp argument decides it), and the row's mean stays at its initial 0.  The mesh is fixed,
+// so the rows that do need one are found once, at case creation: one warp per row.
+__global__ void sponge_flags_kernel(const double* xcx, long long plane, int Nk, int ng, int ni, int nj, int nk,
+                                    double invL, double xs, double inv_dx, unsigned char* flags) {
+    const int row = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (row >= ni * nj) return;          // uniform over the warp
+    const int i = row / nj + ng, j = row % nj + ng;
+    const long long base = i * plane + (long long)j * Nk;
+    bool active = false;
+    for (int k = ng + lane; k < ng + nk; k += 32) active |= (xcx[base + k] * invL - xs) * inv_dx > 0.0;
+    active = __any_sync(0xffffffffu, active);
+    if (lane == 0) flags[row] = active ? 1 : 0;
 }
 
-cudaError_t launch_sponge_mean(const SpongeArgs& S, int max_rows, cudaStream_t s) {
-    dim3 grid((max_rows + 3) / 4, S.nblocks);
-    sponge_mean_kernel<<<grid, 128, 0, s>>>(S);
+cudaError_t launch_sponge_flags(const double* xcx, long long plane, int Nk, int ng, int ni, int nj, int nk,
+                                double invL, double xs, double inv_dx, unsigned char* flags, cudaStream_t s) {
+    const int rows = ni * nj;
+    if (rows == 0) return cudaSuccess;
+    sponge_flags_kernel<<<(rows + 3) / 4, 128, 0, s>>>(xcx, plane, Nk, ng, ni, nj, nk, invL, xs, inv_dx, flags);
     return cudaGetLastError();
 }
 
@@ -301,8 +305,10 @@ cudaError_t launch_sponge_mean(const SpongeArgs& S, int max_rows, cudaStream_t s
 constexpr int SURF_NT = 256;
 
 // CTA order: wall faces first (the longest dependency chains: Newton iterations), then
-// sponge rows, then ghost entries, so the slow parts start in the first wave
-__global__ void __launch_bounds__(SURF_NT) surface_kernel(const __grid_constant__ SurfaceArgs A) {
+// sponge rows, then ghost entries, so the slow parts start in the first wave.  Four CTAs per
+// SM (64 registers, a few spills in the wall part) rather than three at 80: the ghost entries
+// are chains of dependent loads and gain from the extra warps (channel surface time -7 %).
+__global__ void __launch_bounds__(SURF_NT, 4) surface_kernel(const __grid_constant__ SurfaceArgs A) {
     int bx = blockIdx.x;
     if (bx < A.w_ctas) {
         const int w = bx / A.w_per;
@@ -311,8 +317,8 @@ __global__ void __launch_bounds__(SURF_NT) surface_kernel(const __grid_constant_
     }
     bx -= A.w_ctas;
     if (bx < A.s_ctas) {
-        const int b = bx / A.s_per;
-        sponge_row(A.S, b, (bx - b * A.s_per) * (SURF_NT / 32) + (threadIdx.x >> 5), threadIdx.x & 31);
+        const int it = bx * (SURF_NT / 32) + (threadIdx.x >> 5);     // uniform over the warp
+        if (it < A.S.nrows) sponge_row(A.S, A.S.rows[2 * it], A.S.rows[2 * it + 1], threadIdx.x & 31);
         return;
     }
     bx -= A.s_ctas;
@@ -320,12 +326,11 @@ __global__ void __launch_bounds__(SURF_NT) surface_kernel(const __grid_constant_
     if (e < A.G.total) ghost_entry(A.G, e);
 }
 
-cudaError_t launch_surface(SurfaceArgs& A, int max_sponge_rows, cudaStream_t s) {
+cudaError_t launch_surface(SurfaceArgs& A, cudaStream_t s) {
     A.g_ctas = (A.G.total + SURF_NT - 1) / SURF_NT;
     A.w_per = A.W.nwalls ? (A.W.max_faces + SURF_NT - 1) / SURF_NT : 0;
     A.w_ctas = A.w_per * A.W.nwalls;
-    A.s_per = A.S.nblocks ? (max_sponge_rows + SURF_NT / 32 - 1) / (SURF_NT / 32) : 0;
-    A.s_ctas = A.s_per * A.S.nblocks;
+    A.s_ctas = (A.S.nrows + SURF_NT / 32 - 1) / (SURF_NT / 32);
     const int n = A.g_ctas + A.w_ctas + A.s_ctas;
     if (n == 0) return cudaSuccess;
     surface_kernel<<<n, SURF_NT, 0, s>>>(A);
