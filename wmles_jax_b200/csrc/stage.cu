@@ -50,7 +50,10 @@ constexpr int stage_min_ctas(size_t rsize, int nt) {
 // stage time per step, 8 x 32 tile (config 2 KEP / config 3 / config 4 Hybrid): 3.17 / 3.37 /
 // 3.72 ms at 256 threads (254 registers), 2.81 / 3.08 / 3.74 at 352, 2.65 / 2.81 / 3.20 at
 // 448, 2.67 / 2.78 / 3.03 at 512; 16 x 16 tile: KEP 2.93 at 448 (3.03 at 352), Hybrid
-// 3.12 / 2.61 at 352 (3.17 / 2.77 at 384, 3.52 / 2.85 at 512).  The float form's two-CTA
+// 3.12 / 2.61 at 352 (3.17 / 2.77 at 384, 3.52 / 2.85 at 512).  Since the FP64 form's two
+// phases per plane (below), KEP runs 512 threads as well: 16 warps are charged the registers
+// of 14 (groups of four), and the conversion gets five warps (config 2 stage per step 2.586
+// against 2.598 ms at 448).  The float form's two-CTA
 // tiles (issue-bound rather than latency-bound) gain nothing measurable and keep their
 // columns' threads; its one-CTA 16 x 32 tile runs 640 threads at 96 registers (mixed stage
 // time per step, configs 2 / 3 / 4: 1.52 / 1.23 / 1.14 ms, against 1.65 / 1.36 / 1.23 at
@@ -59,7 +62,7 @@ constexpr int STAGE_MAX_WARPS = 32;          // two reduction sums per warp in t
 constexpr int stage_extra_warps(size_t rsize, int scheme, int tj, int tk) {
     if (rsize == 4) return tj * tk == 512 ? 4 : 0;
     if (tj * tk != 256) return 0;
-    if (scheme == WM_SCHEME_KEP) return 6;
+    if (scheme == WM_SCHEME_KEP) return 8;
     return tj == 8 ? 8 : 3;
 }
 
@@ -298,10 +301,10 @@ __device__ __forceinline__ void stage_segment(const StageArgs& A, const StageOpt
     // ---- gradient records of plane ip and (conv) primitives of plane ip+2 from the staging
     // buffer.  The warps that hold a record take one each; the warps left over convert (at
     // most five cells each, about the time of one record), and the cells beyond their share
-    // go to the record warps after their record.  (The 8 x 32 and 16 x 16 KEP tiles: 96
-    // converting threads, every cell theirs.  Three or four rounds for the converting warps,
-    // the rest on the record warps: 1.1-1.4 % slower on the channel, the same on the ramp and
-    // the C-grid.)
+    // go to the record warps after their record.  (The 8 x 32 tile at 512 threads: 160
+    // converting threads, three rounds.  At 448 threads, 96 converting threads: five rounds
+    // took every cell; three or four rounds with the rest on the record warps were 1.1-1.4 %
+    // slower on the channel, the same on the ramp and the C-grid.)
     auto grad_convert = [&](int ip, bool conv) {
         constexpr int GW = (GN + 31) / 32 * 32;          // threads of the record warps
         constexpr int SP = NTH - GW;                     // threads of the converting warps
