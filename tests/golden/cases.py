@@ -186,14 +186,20 @@ from wmles_jax_b200.workloads import RAMP_H, RAMP_SPAN, RAMP_TOP, ramp_nodes, ra
 
 
 def ramp_case(W, n=(12, 8, 6), scheme_factory=None, sgs="vreman", seed=0, n_modes=16,
-              scales=(0.1, 0.02, 0.03), sponge_start_l=3.0, x_range=(-0.76, 4.0)):
+              scales=(0.1, 0.02, 0.03), sponge_start_l=3.0, x_range=(-0.76, 4.0), skew_z=0.0):
     """Single-block smooth ramp: synthetic inflow (i-min), characteristic outflow (i-max),
-    adiabatic wall model (j-min), slip top (j-max), periodic span; spanwise sponge."""
+    adiabatic wall model (j-min), slip top (j-max), periodic span; spanwise sponge.
+    ``skew_z`` shears the span with height (z += skew_z * y), so that the cell centres' z
+    depends on j as well as k (an inflow plane that is not extruded)."""
     gas = W.Gas()
     props = ramp_props(gas)
     profile = ramp_profile()
     L = props["L"]
-    blk = W.Block("ramp", ramp_nodes(n, x_range=x_range, L=L))
+    nodes = ramp_nodes(n, x_range=x_range, L=L)
+    if skew_z:
+        nodes = nodes.copy()
+        nodes[2] = nodes[2] + skew_z * nodes[1]
+    blk = W.Block("ramp", nodes)
     mesh = W.Mesh([blk])
     mesh.connect(blk, "kmin", blk, "kmax", shift=(0.0, 0.0, -RAMP_SPAN * L))
     prim_inf = np.array([props["rho_inf"], props["U_inf"], 0.0, 0.0, props["p_inf"]])

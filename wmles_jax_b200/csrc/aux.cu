@@ -244,10 +244,12 @@ cudaError_t launch_dt(const DtArgs& D, cudaStream_t s) {
 
 // ------------------------------------------------------------------ synthetic inflow
 // SmoothRampInflow.fill_at_time / _unit_noise (wmles/smooth_ramp.py:150-197), in two
-// launches: the mode sums (n_modes cosines per component and ghost cell) cut into IN_PARTS
-// contiguous mode ranges, one thread per (range, row, component, k), so that no thread
-// evaluates more than n_modes / IN_PARTS cosines; then one CTA per (ghost layer, j) row adds
-// the ranges in order, normalises the row and writes the ghost states.
+// launches.  The mode sums: on a general inflow plane n_modes cosines per component and ghost
+// cell, cut into IN_PARTS contiguous mode ranges, one thread per (range, row, component, k), so
+// that no thread evaluates more than n_modes / IN_PARTS cosines (inflow_modes_kernel); on an
+// extruded plane factored sums, one sincos per (component, mode, row)
+// (inflow_ext_sums_kernel).  Then one CTA per (ghost layer, j) row adds the ranges in order,
+// normalises the row and writes the ghost states (inflow_row_kernel).
 constexpr int IN_NT = 256;
 
 __global__ void __launch_bounds__(IN_NT) inflow_modes_kernel(const __grid_constant__ InflowArgs I, long long units) {
@@ -301,79 +303,205 @@ struct InterpAt {
     }
 };
 
-__global__ void __launch_bounds__(IN_NT) inflow_kernel(const __grid_constant__ InflowArgs I) {
-    extern __shared__ double fsm[];            // 3 x Nk
-    __shared__ double red[IN_NT / 32];
+// time-independent factors of the inflow state per ghost cell (np.interp of the profile table
+// at the cell's y, wmles/smooth_ramp.py:160-169), computed once at case creation:
+// sqrt(uu), l10, l11, sqrt(ww), U * U_mean, U * V_mean
+__global__ void inflow_prof_kernel(const __grid_constant__ InflowArgs I, double* prof, long long n) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;   // ghost-slab cell
+    if (idx >= n) return;
     const BlockDev& B = *I.block;
-    const int ng = B.ng, Nj = B.N[1], Nk = B.N[2], nk = B.n[2];
-    const int j = blockIdx.x, m = blockIdx.y, gi = ng - 1 - m;
-    const long long N = B.ncell;
-    double* f0 = fsm;
-    // raw mode sums of the row's three components: the partial sums added in range order
-    const long long rows = (long long)ng * Nj, row = (long long)m * Nj + j;
-    for (int it = threadIdx.x; it < 3 * Nk; it += IN_NT) {
-        double acc = I.raw[row * 3 * Nk + it];
-        for (int pt = 1; pt < IN_PARTS; ++pt) acc += I.raw[(pt * rows + row) * 3 * Nk + it];
-        fsm[it] = acc;
-    }
-    __syncthreads();
-    for (int c = 0; c < 3; ++c) {
-        double* f = fsm + c * Nk;
-        double s_int = 0.0;
-        for (int k = threadIdx.x; k < Nk; k += IN_NT)
-            if (k >= ng && k < ng + nk) s_int += f[k];
-        const double mean = block_sum<IN_NT>(s_int, red) / nk;
-        double cov_acc = 0.0;
-        for (int k = threadIdx.x; k < Nk; k += IN_NT) {
-            f[k] -= mean;
-            if (c == 1 && k >= ng && k < ng + nk) cov_acc += f[k] * f0[k];
-        }
-        if (c == 1) {
-            const double cov = block_sum<IN_NT>(cov_acc, red) / nk;
-            for (int k = threadIdx.x; k < Nk; k += IN_NT) f[k] -= cov * f0[k];
-        }
-        double v_acc = 0.0;
-        for (int k = threadIdx.x; k < Nk; k += IN_NT)
-            if (k >= ng && k < ng + nk) v_acc += f[k] * f[k];
-        const double var = block_sum<IN_NT>(v_acc, red) / nk;
-        const double inv = 1.0 / sqrt(fmax(var, 1e-20));
-        for (int k = threadIdx.x; k < Nk; k += IN_NT) f[k] *= inv;
-        __syncthreads();
-    }
-    const long long on = (long long)ng * Nj * Nk;
+    const double y = B.met[WM_MET_XCY * B.ncell + idx] / I.L;
+    const InterpAt at(I.table, I.n_tab, y);
     const double U = I.U_inf;
-    for (int k = threadIdx.x; k < Nk; k += IN_NT) {
-        const long long idx = ((long long)gi * Nj + j) * Nk + k;
-        const double y = B.met[WM_MET_XCY * N + idx] / I.L;
-        const InterpAt at(I.table, I.n_tab, y);
-        const double uu = fmax(at.col(I.table, y, 3), 0.0) * (U * U);
-        const double vv = fmax(at.col(I.table, y, 4), 0.0) * (U * U);
-        const double ww = fmax(at.col(I.table, y, 5), 0.0) * (U * U);
-        const double uv = at.col(I.table, y, 6) * (U * U);
-        const double su = sqrt(uu);
-        const double l10 = su > 1e-14 ? uv / fmax(su, 1e-14) : 0.0;
-        const double l11 = sqrt(fmax(vv - l10 * l10, 0.0));
-        const double n0 = fsm[k], n1 = fsm[Nk + k], n2 = fsm[2 * Nk + k];
-        const double u = U * at.col(I.table, y, 1) + su * n0;
-        const double v = U * at.col(I.table, y, 2) + l10 * n0 + l11 * n1;
-        const double w = sqrt(ww) * n2;
-        const double rho = I.rho_inf, p = I.p_inf;
-        I.out[idx] = rho;
-        I.out[on + idx] = rho * u;
-        I.out[2 * on + idx] = rho * v;
-        I.out[3 * on + idx] = rho * w;
-        I.out[4 * on + idx] = p / I.gm1 + 0.5 * rho * ((u * u + v * v) + w * w);
+    const double uu = fmax(at.col(I.table, y, 3), 0.0) * (U * U);
+    const double vv = fmax(at.col(I.table, y, 4), 0.0) * (U * U);
+    const double ww = fmax(at.col(I.table, y, 5), 0.0) * (U * U);
+    const double uv = at.col(I.table, y, 6) * (U * U);
+    const double su = sqrt(uu);
+    const double l10 = su > 1e-14 ? uv / fmax(su, 1e-14) : 0.0;
+    prof[idx] = su;
+    prof[n + idx] = l10;
+    prof[2 * n + idx] = sqrt(fmax(vv - l10 * l10, 0.0));
+    prof[3 * n + idx] = sqrt(ww);
+    prof[4 * n + idx] = U * at.col(I.table, y, 1);
+    prof[5 * n + idx] = U * at.col(I.table, y, 2);
+}
+
+// ghost state of slab cell idx (slab size on) from its profile factors and the unit noise
+// (n0, n1, n2) of its row, wmles/smooth_ramp.py:166-176
+__device__ __forceinline__ void inflow_write(const InflowArgs& I, long long idx, long long on, double n0, double n1,
+                                             double n2) {
+    const double* P = I.prof;
+    const double u = P[4 * on + idx] + P[idx] * n0;
+    const double v = P[5 * on + idx] + P[on + idx] * n0 + P[2 * on + idx] * n1;
+    const double w = P[3 * on + idx] * n2;
+    const double rho = I.rho_inf, p = I.p_inf;
+    I.out[idx] = rho;
+    I.out[on + idx] = rho * u;
+    I.out[2 * on + idx] = rho * v;
+    I.out[3 * on + idx] = rho * w;
+    I.out[4 * on + idx] = p / I.gm1 + 0.5 * rho * ((u * u + v * v) + w * w);
+}
+
+// ---- extruded inflow plane (z a function of k alone, y constant along k on every ghost row):
+// each mode's argument splits as alpha + beta with alpha = (kx X + ky y) + phase per row and
+// beta = kz z per k, so cos(alpha + beta) = cos alpha cos beta - sin alpha sin beta with the
+// beta factors tabulated once (inflow_cz_kernel): a fill takes one sincos per (component,
+// mode, row) instead of one cosine per (component, mode, cell).  The argument is rounded as
+// two parts instead of the reference's one sum, a difference of a few units in the last place
+// of the argument.
+__global__ void inflow_cz_kernel(const __grid_constant__ InflowArgs I, int Nk, double* cz) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nm = I.n_modes;
+    if (t >= 3 * nm * Nk) return;
+    const int k = t % Nk, cq = t / Nk, c = cq / nm, q = cq - c * nm;
+    const BlockDev& B = *I.block;
+    const double z = B.met[WM_MET_XCZ * B.ncell + k] / I.L;      // row (0, 0): every row has this z
+    double sb, cb;
+    sincos(I.modes[(c * 4 + 2) * nm + q] * z, &sb, &cb);
+    cz[t] = cb;
+    cz[3 * nm * Nk + t] = sb;
+}
+
+__device__ __forceinline__ void cp_async8_ca(void* smem, const void* gmem) {
+    const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(a), "l"(gmem) : "memory");
+}
+
+// sum over the 32 lanes, the same value on every lane
+__device__ __forceinline__ double warp_allsum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// mode sums of an extruded plane: CTA (g, c) takes component c of the ghost rows
+// [g * IN_EXT_ROWS, (g + 1) * IN_EXT_ROWS) (row = layer m * Nj + j, as in inflow_modes_kernel);
+// the component's cos / sin (kz z) table is staged in shared memory once, then the rows'
+// sincos of alpha, then one thread per (row, k) dot product over the modes from shared memory.
+// Output: raw[(row * 3 + c) * Nk + k] (one range).
+__global__ void __launch_bounds__(IN_EXT_NT) inflow_ext_sums_kernel(const __grid_constant__ InflowArgs I) {
+    extern __shared__ double sm[];    // cos beta, sin beta: 2 x n_modes x Nk; then cos, sin alpha: rows x 2 x n_modes
+    const BlockDev& B = *I.block;
+    const int ng = B.ng, Nj = B.N[1], Nk = B.N[2];
+    const int c = blockIdx.y, nm = I.n_modes;
+    const int rows = ng * Nj, r0 = blockIdx.x * IN_EXT_ROWS, nr = min(IN_EXT_ROWS, rows - r0);
+    double* tb = sm;
+    double* ta = sm + 2 * nm * Nk;
+    const double* cz = I.cz + (size_t)c * nm * Nk;
+    // the table arrives by cp.async while the sincos below are computed
+    for (int t = threadIdx.x; t < nm * Nk; t += IN_EXT_NT) {
+        cp_async8_ca(tb + t, cz + t);
+        cp_async8_ca(tb + nm * Nk + t, cz + (size_t)3 * nm * Nk + t);
+    }
+    const double time = I.time0 + I.time_dt * (I.dt ? *I.dt : 0.0);
+    const double X = I.U_inf * time / I.L;
+    const double* md = I.modes + c * 4 * nm;
+    for (int t = threadIdx.x; t < nr * nm; t += IN_EXT_NT) {
+        const int rr = t / nm, q = t - rr * nm;
+        const int row = r0 + rr, m = row / Nj, j = row - m * Nj, gi = ng - 1 - m;
+        const double y = B.met[WM_MET_XCY * B.ncell + ((long long)gi * Nj + j) * Nk] / I.L;
+        double s_, c_;
+        sincos((md[q] * X + md[nm + q] * y) + md[3 * nm + q], &s_, &c_);
+        ta[(2 * rr) * nm + q] = c_;
+        ta[(2 * rr + 1) * nm + q] = s_;
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncthreads();
+    for (int t = threadIdx.x; t < nr * Nk; t += IN_EXT_NT) {
+        const int rr = t / Nk, k = t - rr * Nk;
+        const double* ca = ta + 2 * rr * nm;
+        const double* sa = ca + nm;
+        double a0 = 0.0, a1 = 0.0;          // even and odd modes
+        int q = 0;
+        for (; q + 1 < nm; q += 2) {
+            a0 += ca[q] * tb[q * Nk + k] - sa[q] * tb[(nm + q) * Nk + k];
+            a1 += ca[q + 1] * tb[(q + 1) * Nk + k] - sa[q + 1] * tb[(nm + q + 1) * Nk + k];
+        }
+        if (q < nm) a0 += ca[q] * tb[q * Nk + k] - sa[q] * tb[(nm + q) * Nk + k];
+        I.raw[((long long)(r0 + rr) * 3 + c) * Nk + k] = a0 + a1;
     }
 }
 
+// one ghost row (layer m, j) of any plane: the raw mode sums (parts ranges, added in range
+// order), the row's normalisation of wmles/smooth_ramp.py:186-196 by warp c for component c
+// (warp sums; component 1 takes component 0's final values after a barrier), the ghost states
+__global__ void __launch_bounds__(IN_ROW_NT) inflow_row_kernel(const __grid_constant__ InflowArgs I, int parts) {
+    extern __shared__ double sm[];          // noise: 3 x Nk
+    const BlockDev& B = *I.block;
+    const int ng = B.ng, Nj = B.N[1], Nk = B.N[2], nk = B.n[2];
+    const int j = blockIdx.x, m = blockIdx.y, gi = ng - 1 - m;
+    const int c = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long rows = (long long)ng * Nj, row = (long long)m * Nj + j;
+    double* f = sm + c * Nk;
+    for (int k = lane; k < Nk; k += 32) {
+        double acc = I.raw[(row * 3 + c) * Nk + k];
+        for (int pt = 1; pt < parts; ++pt) acc += I.raw[((pt * rows + row) * 3 + c) * Nk + k];
+        f[k] = acc;
+    }
+    __syncwarp();
+    double s_int = 0.0;
+    for (int k = ng + lane; k < ng + nk; k += 32) s_int += f[k];
+    const double mean = warp_allsum(s_int) / nk;
+    for (int k = lane; k < Nk; k += 32) f[k] -= mean;
+    __syncwarp();
+    auto normalise = [&]() {
+        double v_acc = 0.0;
+        for (int k = ng + lane; k < ng + nk; k += 32) v_acc += f[k] * f[k];
+        const double inv = 1.0 / sqrt(fmax(warp_allsum(v_acc) / nk, 1e-20));
+        for (int k = lane; k < Nk; k += 32) f[k] *= inv;
+    };
+    if (c != 1) normalise();
+    __syncthreads();
+    if (c == 1) {
+        const double* f0 = sm;
+        double cov_acc = 0.0;
+        for (int k = ng + lane; k < ng + nk; k += 32) cov_acc += f[k] * f0[k];
+        const double cov = warp_allsum(cov_acc) / nk;
+        for (int k = lane; k < Nk; k += 32) f[k] -= cov * f0[k];
+        __syncwarp();
+        normalise();
+    }
+    __syncthreads();
+    const long long row0 = ((long long)gi * Nj + j) * Nk;
+    for (int k = threadIdx.x; k < Nk; k += IN_ROW_NT)
+        inflow_write(I, row0 + k, (long long)ng * Nj * Nk, sm[k], sm[Nk + k], sm[2 * Nk + k]);
+}
+
+cudaError_t launch_inflow_setup(const InflowArgs& I, int Nj, int Nk, int ng, double* prof, double* cz, cudaStream_t s) {
+    const long long n = (long long)ng * Nj * Nk;
+    inflow_prof_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(I, prof, n);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || cz == nullptr) return e;
+    const int t = 3 * I.n_modes * Nk;
+    inflow_cz_kernel<<<(t + 255) / 256, 256, 0, s>>>(I, Nk, cz);
+    return cudaGetLastError();
+}
+
+size_t inflow_ext_smem(int n_modes, int Nk) {
+    return sizeof(double) * (2 * (size_t)n_modes * Nk + 2 * (size_t)IN_EXT_ROWS * n_modes);
+}
+
 cudaError_t launch_inflow(const InflowArgs& I, int Nj, int Nk, int ng, cudaStream_t s) {
-    const long long units = (long long)IN_PARTS * ng * Nj * 3 * Nk;
-    inflow_modes_kernel<<<(unsigned)((units + IN_NT - 1) / IN_NT), IN_NT, 0, s>>>(I, units);
+    int parts = IN_PARTS;
+    if (I.cz != nullptr) {
+        const size_t sm = inflow_ext_smem(I.n_modes, Nk);
+        static bool attr = false;     // the attribute is set once per process
+        if (!attr) {
+            const cudaError_t e = cudaFuncSetAttribute(inflow_ext_sums_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       (int)inflow_ext_smem_max());
+            if (e != cudaSuccess) return e;
+            attr = true;
+        }
+        inflow_ext_sums_kernel<<<dim3((ng * Nj + IN_EXT_ROWS - 1) / IN_EXT_ROWS, 3), IN_EXT_NT, sm, s>>>(I);
+        parts = 1;
+    } else {
+        const long long units = (long long)IN_PARTS * ng * Nj * 3 * Nk;
+        inflow_modes_kernel<<<(unsigned)((units + IN_NT - 1) / IN_NT), IN_NT, 0, s>>>(I, units);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    dim3 grid(Nj, ng);
-    const size_t sm = sizeof(double) * 3 * Nk;
-    inflow_kernel<<<grid, IN_NT, sm, s>>>(I);
+    inflow_row_kernel<<<dim3(Nj, ng), IN_ROW_NT, sizeof(double) * 3 * Nk, s>>>(I, parts);
     return cudaGetLastError();
 }
 

@@ -105,12 +105,23 @@ struct InflowArgs {
     const double* dt;
     double* raw;             // IN_PARTS x (ng * Nj) x 3 x Nk partial mode sums (scratch)
     double* out;             // 5 x (ng * Nj * Nk)
+    const double* prof;      // 6 x (ng * Nj * Nk): the time-independent profile factors per ghost cell
+    const double* cz;        // extruded plane: cos(kz z), then sin(kz z), each 3 x n_modes x Nk;
+                             // null: general plane (direct cosines)
 };
 
 // partial mode sums per (component, cell) of the synthetic inflow (contiguous mode ranges)
 constexpr int IN_PARTS = 4;
-// kernel launches of one inflow fill
+// kernel launches of one inflow fill (mode sums, then the rows)
 constexpr int IN_LAUNCHES = 2;
+// the rows' launch: one warp per velocity component of a ghost row
+constexpr int IN_ROW_NT = 96;
+// extruded plane: ghost rows per CTA of the mode sums, threads per CTA, and the largest
+// dynamic shared memory of that launch (one component's cos / sin (kz z) table and the rows'
+// sincos of alpha)
+constexpr int IN_EXT_ROWS = 4, IN_EXT_NT = 256;
+constexpr size_t inflow_ext_smem_max() { return 200 * 1024; }
+size_t inflow_ext_smem(int n_modes, int Nk);
 
 // before each stage kernel: ghost gather (single phase), wall model and sponge means in one
 // launch; the CTA counts are filled in by the launcher (an empty part has none)
@@ -145,5 +156,8 @@ cudaError_t launch_status_gather(const CaseDev* cases, int ncases, unsigned* out
 cudaError_t launch_sponge_flags(const double* xcx, long long plane, int Nk, int ng, int ni, int nj, int nk,
                                 double invL, double xs, double inv_dx, unsigned char* flags, cudaStream_t s);
 cudaError_t launch_inflow(const InflowArgs& I, int Nj, int Nk, int ng, cudaStream_t s);
+// set-up of a case's inflow: prof (always) and, for an extruded plane, cz (I.prof, I.cz are
+// the destinations here)
+cudaError_t launch_inflow_setup(const InflowArgs& I, int Nj, int Nk, int ng, double* prof, double* cz, cudaStream_t s);
 
 }  // namespace wm

@@ -154,6 +154,9 @@ struct wm_case {
     bool has_inflow = false;
     int inflow_block = -1;
     double *d_modes = nullptr, *d_table = nullptr, *inflow_buf = nullptr, *inflow_raw = nullptr;
+    double* inflow_prof = nullptr;       // 6 x inflow_n time-independent profile factors
+    double* inflow_cz = nullptr;         // extruded inflow plane: cos / sin (kz z) tables (else null)
+    BlockDev* d_inflow_block = nullptr;  // the inflow block's descriptor, for the set-up kernels
     wm_inflow inflow{};
     long long inflow_n = 0;
     std::vector<double*> spmean;         // per block, null without sponge
@@ -534,6 +537,8 @@ int fill_inflow(View* v, Prof* pf, const double* times, double time_dt, const do
         I.time0 = times[ci]; I.time_dt = time_dt; I.dt = dt ? dt[ci] : nullptr;
         I.raw = c->inflow_raw;
         I.out = c->inflow_buf;
+        I.prof = c->inflow_prof;
+        I.cz = c->inflow_cz;
         LaunchScope ls(pf, WM_KIND_SOURCE, s, IN_LAUNCHES);
         CK(launch_inflow(I, B.N[1], B.N[2], B.ng, s));
     }
@@ -798,6 +803,29 @@ int wm_case_create(const wm_case_desc* d, wm_case** out) {
         c->inflow_n = (long long)B.ng * B.plane;
         if ((r = c->mem.alloc(&c->inflow_buf, 5 * (size_t)c->inflow_n))) return bail(r);
         if ((r = c->mem.alloc(&c->inflow_raw, (size_t)IN_PARTS * 3 * c->inflow_n))) return bail(r);
+        if ((r = c->mem.alloc(&c->inflow_prof, 6 * (size_t)c->inflow_n))) return bail(r);
+        if ((r = c->mem.upload(&c->d_inflow_block, &B, 1))) return bail(r);
+        // extruded plane: every ghost row's y constant along k, z the same function of k on
+        // every row (then the mode sums factor per row and per k); one component's cos / sin
+        // (kz z) table must fit the mode-sum launch's shared memory
+        const size_t n = (size_t)c->inflow_n;
+        std::vector<double> y(n), z(n);
+        CKB(cudaMemcpy(y.data(), B.met + (size_t)WM_MET_XCY * B.ncell, sizeof(double) * n, cudaMemcpyDeviceToHost));
+        CKB(cudaMemcpy(z.data(), B.met + (size_t)WM_MET_XCZ * B.ncell, sizeof(double) * n, cudaMemcpyDeviceToHost));
+        const int Nk = B.N[2];
+        bool extruded = inflow_ext_smem(I.n_modes, Nk) <= inflow_ext_smem_max();
+        for (size_t cell = 0; cell < n && extruded; ++cell) {
+            const size_t k = cell % Nk;
+            extruded = y[cell] == y[cell - k] && z[cell] == z[k];
+        }
+        InflowArgs IA{};
+        IA.block = c->d_inflow_block;
+        IA.modes = c->d_modes; IA.table = c->d_table;
+        IA.n_modes = I.n_modes; IA.n_tab = I.n_tab;
+        IA.U_inf = I.U_inf; IA.L = I.L;
+        if (extruded)
+            if ((r = c->mem.alloc(&c->inflow_cz, 2 * 3 * (size_t)I.n_modes * Nk))) return bail(r);
+        CKB(launch_inflow_setup(IA, B.N[1], Nk, B.ng, c->inflow_prof, c->inflow_cz, 0));
     }
 
     // ---- sponge means
