@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(DT_NT) dt_kernel(const __grid_constant__ DtArg
             for (int v = 0; v < 5; ++v) qv[v] = q[v * N + idx];
             // every metric this cell needs, read-only and issued before any store to q
             const long long off[3] = {plane, Nk, 1};
-            double Sl[9], Sh[9];
+            M Sl[9], Sh[9];
 #pragma unroll
             for (int d = 0; d < 3; ++d)
 #pragma unroll
@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(DT_NT) dt_kernel(const __grid_constant__ DtArg
                     Sl[3 * d + x] = __ldg(met + (3 * d + x) * N + idx);
                     Sh[3 * d + x] = __ldg(met + (3 * d + x) * N + idx + off[d]);
                 }
-            const double vol = __ldg(met + WM_MET_VOL * N + idx);
+            const M vol = __ldg(met + WM_MET_VOL * N + idx);
             if (cmf) {
                 const double delta = D.cmf_delta[B.case_id];
                 const int m = 1 + C.cmf_dir;
@@ -137,21 +137,28 @@ __global__ void __launch_bounds__(DT_NT) dt_kernel(const __grid_constant__ DtArg
                 if (bad) atomicOr(C.status, bad);
             }
             if (D.want_dt) {
-                const double ivol = 1.0 / vol;
-                const double T = p * ir * C.inv_Rg;
-                const double cs = sqrt(C.gamma * C.Rg * T);
-                const double nu = C.nu_fac * sutherland_d(T, C) * ir;
-                double lam = 0.0, lamv = 0.0;
+                // the cell's CFL rate in the metric precision: FP64 in the FP64 form; FP32 in the
+                // mixed form, from its FP32 metric copy like its fluxes (the state, its checks,
+                // the constraint and the minimum over cells stay FP64)
+                using CF = M;
+                const CF ivol = CF(1) / vol;
+                const CF irc = CF(ir);
+                const CF T = CF(p) * irc * CF(C.inv_Rg);
+                const CF cs = sqrt(CF(C.gamma) * CF(C.Rg) * T);
+                const CF x = T * CF(C.inv_Tref);
+                const CF nu = CF(C.nu_fac) * (CF(C.mu_ref) * (x * sqrt(x)) * CF(C.TrefS) / (T + CF(C.S_suth))) * irc;
+                const CF uc = CF(u), vc = CF(v), wc = CF(w);
+                CF lam = CF(0), lamv = CF(0);
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
-                    const double sx = 0.5 * (Sl[3 * d] + Sh[3 * d]);
-                    const double sy = 0.5 * (Sl[3 * d + 1] + Sh[3 * d + 1]);
-                    const double sz = 0.5 * (Sl[3 * d + 2] + Sh[3 * d + 2]);
-                    const double Sm = sqrt((sx * sx + sy * sy) + sz * sz);
-                    lam = lam + fabs((u * sx + v * sy) + w * sz) + cs * Sm;
+                    const CF sx = CF(0.5) * (Sl[3 * d] + Sh[3 * d]);
+                    const CF sy = CF(0.5) * (Sl[3 * d + 1] + Sh[3 * d + 1]);
+                    const CF sz = CF(0.5) * (Sl[3 * d + 2] + Sh[3 * d + 2]);
+                    const CF Sm = sqrt((sx * sx + sy * sy) + sz * sz);
+                    lam = lam + fabs((uc * sx + vc * sy) + wc * sz) + cs * Sm;
                     lamv = lamv + nu * (Sm * Sm) * ivol;
                 }
-                run = nanmin(run, C.cfl * vol / (lam + 4.0 * lamv));
+                run = nanmin(run, double(CF(C.cfl) * vol / (lam + CF(4) * lamv)));
             }
         }
     }
