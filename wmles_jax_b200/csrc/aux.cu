@@ -493,13 +493,12 @@ cudaError_t launch_inflow(const InflowArgs& I, int Nj, int Nk, int ng, cudaStrea
     int parts = IN_PARTS;
     if (I.cz != nullptr) {
         const size_t sm = inflow_ext_smem(I.n_modes, Nk);
-        static bool attr = false;     // the attribute is set once per process
-        if (!attr) {
-            const cudaError_t e = cudaFuncSetAttribute(inflow_ext_sums_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                       (int)inflow_ext_smem_max());
-            if (e != cudaSuccess) return e;
-            attr = true;
-        }
+        static std::atomic<unsigned long long> attr{0};     // one bit per device
+        const cudaError_t e = once_per_device(attr, [] {
+            return cudaFuncSetAttribute(inflow_ext_sums_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)inflow_ext_smem_max());
+        });
+        if (e != cudaSuccess) return e;
         inflow_ext_sums_kernel<<<dim3((ng * Nj + IN_EXT_ROWS - 1) / IN_EXT_ROWS, 3), IN_EXT_NT, sm, s>>>(I);
         parts = 1;
     } else {

@@ -659,14 +659,11 @@ __global__ void __launch_bounds__(StageLayout<R, SCHEME, TJ, TK>::NTH, StageLayo
 template <typename R, int SCHEME, int TJ, int TK>
 static cudaError_t configure_one() {
     using LY = StageLayout<R, SCHEME, TJ, TK>;
-    static bool done = false;     // per instantiation; the attribute is set once per process
-    if (!done) {
-        cudaError_t e = cudaFuncSetAttribute(stage_kernel<R, SCHEME, TJ, TK>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LY::bytes);
-        if (e != cudaSuccess) return e;
-        done = true;
-    }
-    return cudaSuccess;
+    static std::atomic<unsigned long long> done{0};     // per instantiation, one bit per device
+    return once_per_device(done, [] {
+        return cudaFuncSetAttribute(stage_kernel<R, SCHEME, TJ, TK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)LY::bytes);
+    });
 }
 
 template <typename R, int SCHEME, int TJ, int TK>

@@ -4,11 +4,27 @@
 // per-case constants, wall faces and stage tiles are concatenated into device tables.
 // Blocks carry a global index (into the view's block table) and their case's index.
 #pragma once
+#include <atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 #include "../../include/wmles_cuda.h"
 
 namespace wm {
+
+// runs `set` (a kernel attribute set-up, which holds for the current device only) once per
+// device: `done` keeps one bit per device ordinal below 64 (others set it on every call); two
+// threads racing on a device both set the same value
+template <class F>
+inline cudaError_t once_per_device(std::atomic<unsigned long long>& done, F set) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = dev >= 0 && dev < 64 ? 1ull << dev : 0ull;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+    e = set();
+    if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_acq_rel);
+    return e;
+}
 
 constexpr int MAX_CASES = WM_MAX_BLOCKS;   // a case has at least one block
 
