@@ -16,7 +16,8 @@
 //   1. gradient records of plane i; the warps without a record convert the staged plane
 //      i+2 to primitives
 //   2. own i-face flux -> RK epilogue of plane i-1; all j/k faces of plane i (flat loop);
-//      the cp.async of plane i+3 is in flight meanwhile
+//      the cp.async of plane i+3 is in flight meanwhile (KEP: the epilogue of plane i-1 runs
+//      in the next phase 1 instead, on the warps without a gradient record)
 // (float form, or several CTAs per SM: three phases, the conversion of plane i+1 first and
 // on its own).
 // Each face flux is evaluated once; each conservative value is read from HBM about once
@@ -88,12 +89,18 @@ struct StageLayout {
     // three phases.
     static constexpr bool FUSE = MIN_CTAS == 1 && sizeof(R) == 8;
     static constexpr int NSLOT = FUSE ? 5 : 4;
+    // KEP in the two-phase form: the RK epilogue deferred to the next gradient phase (below).
+    // Config 2 stage per step 2.546 ms against 2.583; the Hybrid kernels, whose gradient phase
+    // is the longer one, lose with it (ramp +0.5 %, C-grid +6.4 %) and keep it in the face phase.
+    static constexpr bool DEFER = FUSE && SCHEME == WM_SCHEME_KEP;
     static constexpr size_t qs_off = 0;                                        // double [5][PN]
     static constexpr size_t pr_off = qs_off + sizeof(double) * 5 * PN;         // R [NSLOT][PR_N][PN]
     static constexpr size_t gs_off = pr_off + sizeof(R) * NSLOT * PR_N * PN;   // R [NGS][GN]
     static constexpr size_t fj_off = gs_off + sizeof(R) * NGS * GN;            // R [5][FJN]
     static constexpr size_t fk_off = fj_off + sizeof(R) * 5 * FJN;             // R [5][FKN]
-    static constexpr size_t red_off = (fk_off + sizeof(R) * 5 * FKN + 15) / 16 * 16;
+    // deferred epilogue: the flux divergence of the output plane per tile column
+    static constexpr size_t fr_off = fk_off + sizeof(R) * 5 * FKN;            // R [5][NT]
+    static constexpr size_t red_off = (fr_off + (DEFER ? sizeof(R) * 5 * NT : 0) + 15) / 16 * 16;
     static constexpr size_t bytes = red_off + sizeof(double) * 2 * STAGE_MAX_WARPS;
     static_assert(NTH / 32 <= STAGE_MAX_WARPS, "the reduction scratch holds two sums per warp");
     static_assert(!FUSE || GN <= NTH, "the fused phase computes one gradient record per thread");
@@ -192,6 +199,7 @@ __device__ __forceinline__ void stage_segment(const StageArgs& A, const StageOpt
     R* gs = reinterpret_cast<R*>(smem_raw + LY::gs_off);
     R* fj = reinterpret_cast<R*>(smem_raw + LY::fj_off);
     R* fk = reinterpret_cast<R*>(smem_raw + LY::fk_off);
+    R* fr = reinterpret_cast<R*>(smem_raw + LY::fr_off);
     double* red = reinterpret_cast<double*>(smem_raw + LY::red_off);
 
     const BlockDev B = A.blocks[t.blk];
@@ -469,13 +477,14 @@ __device__ __forceinline__ void stage_segment(const StageArgs& A, const StageOpt
         cmf_col = A.cmf_part + A.cmf_slot_start[t.blk] + (long long)col * B.n[0];
     }
 
-    // ---- RK epilogue of interior cell (io, j, k): r = -(div F)/V (+ source), stage update
-    auto output = [&](int io, const R Fhi[5]) {
-        const int idx = io * planei + j * Nk + k;
+    // ---- RK epilogue of interior cell (io, jj, kk) from its flux divergence dv (times -1, not
+    // yet divided by V): r = -(div F)/V (+ source), stage update
+    auto output = [&](int io, int jj, int kk, const R dv[5]) {
+        const int idx = io * planei + jj * Nk + kk;
         const R ivol = __ldg(MB + WM_MET_IVOL * nc + idx);
         R r[5];
 #pragma unroll
-        for (int v = 0; v < 5; ++v) r[v] = ((-(Fhi[v] - Flo[v]) - dFj[v]) - dFk[v]) * ivol;
+        for (int v = 0; v < 5; ++v) r[v] = dv[v] * ivol;
         double rq[5], qi[5];
 #pragma unroll
         for (int v = 0; v < 5; ++v) qi[v] = __ldg(SP.q_in + v * nc + idx);
@@ -484,7 +493,7 @@ __device__ __forceinline__ void stage_segment(const StageArgs& A, const StageOpt
             const double xl = __ldg(B.met + WM_MET_XCX * nc + idx) * C.sp_invL;
             const double eta = fmin(fmax((xl - C.sp_xs) * C.sp_inv_dx, 0.0), 1.0);
             const double sig = C.sp_sigma0 * (eta * eta * eta * (10.0 + eta * (-15.0 + 6.0 * eta)));
-            const long long mi = (long long)io * Nj + j;
+            const long long mi = (long long)io * Nj + jj;
             const long long mn = (long long)B.N[0] * Nj;
 #pragma unroll
             for (int v = 0; v < 5; ++v) rq[v] = double(r[v]) - sig * (qi[v] - SP.spmean[v * mn + mi]);
@@ -518,8 +527,8 @@ __device__ __forceinline__ void stage_segment(const StageArgs& A, const StageOpt
     // 2.62; the Hybrid kernels (ramp, C-grid), which spill more, lose 1-2 % to the extra L1
     // lines.  Loading these values into registers ahead of the flux instead spills more and is
     // slower in every case.
-    auto prefetch_epilogue = [&](int io) {
-        const int idx = io * planei + j * Nk + k;
+    auto prefetch_epilogue = [&](int io, int jj, int kk) {
+        const int idx = io * planei + jj * Nk + kk;
         prefetch_l1(MB + WM_MET_IVOL * nc + idx);
 #pragma unroll
         for (int v = 0; v < 5; ++v) prefetch_l1(SP.q_in + v * nc + idx);
@@ -527,6 +536,45 @@ __device__ __forceinline__ void stage_segment(const StageArgs& A, const StageOpt
 #pragma unroll
             for (int v = 0; v < 5; ++v) prefetch_l1(SP.q0 + v * nc + idx);
         if (cmf_on) prefetch_l1(B.met + WM_MET_VOL * nc + idx);
+    };
+
+    // ---- deferred epilogue (KEP, FP64 two-phase form): the RK epilogue of plane io runs in the
+    // gradient phase of the plane after next (its flux divergence waits in fr), on the warps
+    // that hold no gradient record (on every thread when there are none), so that the face
+    // phase is no longer set by the column threads' i-face flux + epilogue + j/k face; stage
+    // 3's rho u_dir V of the plane is summed per warp into red
+    constexpr int EGW = (GN + 31) / 32 * 32, ESP = NTH - EGW;
+    auto epi_cells = [&](auto&& f) {
+        if constexpr (ESP >= 32) {
+            if (tid >= EGW)
+                for (int c = tid - EGW; c < NT; c += ESP) f(c);
+        } else {
+            for (int c = tid; c < NT; c += NTH) f(c);
+        }
+    };
+    auto epilogue_plane = [&](int io) {
+        epi_cells([&](int c) {
+            const int jj = t.j0 + c / TK, kk = t.k0 + c % TK;
+            if (jj < jhi && kk < khi) {
+                R dv[5];
+#pragma unroll
+                for (int v = 0; v < 5; ++v) dv[v] = fr[v * NT + c];
+                output(io, jj, kk, dv);
+            }
+        });
+        if (cmf_on) {
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) cmf_acc += __shfl_down_sync(0xffffffffu, cmf_acc, off);
+            if ((tid & 31) == 0) red[tid >> 5] = cmf_acc;
+            cmf_acc = 0.0;
+        }
+    };
+    auto cmf_store = [&](int io) {      // after the barrier that follows epilogue_plane(io)
+        if (cmf_on && tid == 0) {
+            double sp = 0.0;
+            for (int w = 0; w < NTH / 32; ++w) sp += red[w];
+            cmf_col[io - ng] = sp;
+        }
     };
 
     // ---- prologue: planes i0-2 .. i0+1 (and i0+2 when fused), gradients of i0-1 and i0,
@@ -560,7 +608,11 @@ __device__ __forceinline__ void stage_segment(const StageArgs& A, const StageOpt
     for (int ip = i0 + 1; ip <= i1; ++ip) {
         if constexpr (LY::FUSE) {
             grad_convert(ip, ip < i1);   // records of plane ip; staged plane ip+2 -> primitives
+            if constexpr (LY::DEFER)
+                if (ip - 2 >= i0) epilogue_plane(ip - 2);
             __syncthreads();
+            if constexpr (LY::DEFER)
+                if (ip - 2 >= i0) cmf_store(ip - 2);
             if (ip + 3 <= i1 + 1) stage_plane(ip + 3);
         } else {
             convert_plane(ip + 1);       // staged plane ip+1 -> primitives
@@ -569,18 +621,33 @@ __device__ __forceinline__ void stage_segment(const StageArgs& A, const StageOpt
             __syncthreads();
             if (ip + 2 <= i1 + 1) stage_plane(ip + 2);
         }
-        if constexpr (SCHEME == WM_SCHEME_KEP)
-            if (active) prefetch_epilogue(ip - 1);
+        if constexpr (SCHEME == WM_SCHEME_KEP) {
+            if constexpr (LY::DEFER) {
+                epi_cells([&](int c) {
+                    const int jj = t.j0 + c / TK, kk = t.k0 + c % TK;
+                    if (jj < jhi && kk < khi) prefetch_epilogue(ip - 1, jj, kk);
+                });
+            } else if (active) {
+                prefetch_epilogue(ip - 1, j, k);
+            }
+        }
         if (ip < i1) prefetch_next(ip);
         if (active) {
-            R Fhi[5];
+            R Fhi[5], dv[5];
             iface_flux(ip, Fhi);
-            output(ip - 1, Fhi);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) dv[v] = (-(Fhi[v] - Flo[v]) - dFj[v]) - dFk[v];
+            if constexpr (LY::DEFER) {
+#pragma unroll
+                for (int v = 0; v < 5; ++v) fr[v * NT + tid] = dv[v];
+            } else {
+                output(ip - 1, j, k, dv);
+            }
 #pragma unroll
             for (int v = 0; v < 5; ++v) Flo[v] = Fhi[v];
         }
         if constexpr (LY::FUSE) save_gs();
-        if (cmf_on) {
+        if (!LY::DEFER && cmf_on) {
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) cmf_acc += __shfl_down_sync(0xffffffffu, cmf_acc, off);
             // warp sums of this plane; two buffers by plane parity (read after the barrier below)
@@ -591,7 +658,7 @@ __device__ __forceinline__ void stage_segment(const StageArgs& A, const StageOpt
             for (int f = rtid; f < LY::FJN + LY::FKN; f += NTH) jk_face(ip, f);
         cp_async_wait_all();
         __syncthreads();
-        if (cmf_on && tid == 0) {
+        if (!LY::DEFER && cmf_on && tid == 0) {
             double sp = 0.0;
             for (int w = 0; w < NTH / 32; ++w) sp += red[(ip & 1) * (NTH / 32) + w];
             cmf_col[ip - 1 - ng] = sp;
@@ -601,7 +668,13 @@ __device__ __forceinline__ void stage_segment(const StageArgs& A, const StageOpt
             if constexpr (!LY::FUSE) save_gs();
         }
     }
-
+    if constexpr (LY::DEFER) {
+        epilogue_plane(i1 - 1);          // the segment's last plane
+        if (cmf_on) {
+            __syncthreads();
+            cmf_store(i1 - 1);
+        }
+    }
 }
 
 template <typename R, int SCHEME, int TJ, int TK>
