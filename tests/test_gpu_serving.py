@@ -100,11 +100,13 @@ def test_server_admission_budget():
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
 def test_results_do_not_depend_on_chunk(precision):
     """The stage work list may be cut into any chunk length along i (a batch picks its own):
-    the constant-mass-flux partials are per column and plane, so results are bit-identical."""
+    the constant-mass-flux partials are per column and plane, so results are bit-identical.
+    Chunks of one and two planes make every segment a prologue, one or two marching steps and
+    the segment's closing epilogue."""
     from wmles_jax_b200 import Solver
     from wmles_jax_b200.workloads import serving_case
     outs = []
-    for chunk in (None, 4, 7, 24):
+    for chunk in (None, 1, 2, 4, 7, 24):
         # a fresh builder per run: prim_fn draws its noise from a generator it owns
         mesh, gas, kw, prim = serving_case(1500.0, 0.3, (24, 16, 16), seed=5)
         s = Solver(mesh, gas, precision=precision, chunk=chunk, **kw)
