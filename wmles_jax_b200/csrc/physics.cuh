@@ -174,24 +174,22 @@ __device__ __forceinline__ R sgs_nut(int model, const R g[9], R delta, R c) {
         return cd * cd * wm_sqrt(R(2) * ss);
     }
     if (model == WM_SGS_WALE) {
-        R ss = R(0), g2[9];
+        // S_ij S_ij and S^d_ij S^d_ij from the six distinct entries of each symmetric tensor
+        // (off-diagonal squares counted twice, an exact doubling), summed as trees: the
+        // reference's contractions up to the order of the additions, with dependency chains
+        // of four additions instead of nine
+        R g2[9];
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                const R s = R(0.5) * (g[3 * i + j] + g[3 * j + i]);
-                ss += s * s;
+            for (int j = 0; j < 3; ++j)
                 g2[3 * i + j] = g[3 * i] * g[j] + g[3 * i + 1] * g[3 + j] + g[3 * i + 2] * g[6 + j];
-            }
+        const R s01 = R(0.5) * (g[1] + g[3]), s02 = R(0.5) * (g[2] + g[6]), s12 = R(0.5) * (g[5] + g[7]);
+        const R ss = ((g[0] * g[0] + g[4] * g[4]) + g[8] * g[8]) + R(2) * ((s01 * s01 + s02 * s02) + s12 * s12);
         const R tr = (g2[0] + g2[4] + g2[8]) * R(1.0 / 3.0);
-        R sdsd = R(0);
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                const R s = R(0.5) * (g2[3 * i + j] + g2[3 * j + i]) - (i == j ? tr : R(0));
-                sdsd += s * s;
-            }
+        const R d0 = g2[0] - tr, d1 = g2[4] - tr, d2 = g2[8] - tr;
+        const R q01 = R(0.5) * (g2[1] + g2[3]), q02 = R(0.5) * (g2[2] + g2[6]), q12 = R(0.5) * (g2[5] + g2[7]);
+        const R sdsd = ((d0 * d0 + d1 * d1) + d2 * d2) + R(2) * ((q01 * q01 + q02 * q02) + q12 * q12);
         const R cd = c * delta;
         const R rsd = wm_sqrt(sdsd), rss = wm_sqrt(ss);
         return cd * cd * (sdsd * rsd) / (ss * ss * rss + sdsd * wm_sqrt(rsd) + R(1e-30));
