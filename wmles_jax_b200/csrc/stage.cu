@@ -271,24 +271,26 @@ __device__ __forceinline__ void stage_segment(const StageArgs& A, const StageOpt
             const R Hjx = __ldg(mj + WM_MET_SJX * nc), Hjy = __ldg(mj + WM_MET_SJY * nc), Hjz = __ldg(mj + WM_MET_SJZ * nc);
             const R Skx = __ldg(m + WM_MET_SKX * nc), Sky = __ldg(m + WM_MET_SKY * nc), Skz = __ldg(m + WM_MET_SKZ * nc);
             const R Hkx = __ldg(mk + WM_MET_SKX * nc), Hky = __ldg(mk + WM_MET_SKY * nc), Hkz = __ldg(mk + WM_MET_SKZ * nc);
-            // half of 1/V: the record holds half the gradient (faces average two records by
-            // adding them); the SGS models are homogeneous of degree one in the gradient and
-            // the Ducros sensor of degree zero, so they take the half gradient directly
-            const R hivol = R(0.5) * __ldg(m + WM_MET_IVOL * nc);
+            // a quarter of 1/V: the face values below are sums of two cells, twice the face
+            // averages (scaling by two is exact, so the products and sums are the averages'
+            // bit for bit, doubled), and the record holds half the gradient (faces average two
+            // records by adding them); the SGS models are homogeneous of degree one in the
+            // gradient and the Ducros sensor of degree zero, so they take the half gradient
+            const R qivol = R(0.25) * __ldg(m + WM_MET_IVOL * nc);
             const R delta = sgs_model != WM_SGS_NONE ? __ldg(m + WM_MET_DELTA * nc) : R(0);
             R acc[12];
 #pragma unroll
             for (int a = 0; a < 4; ++a) {
                 const R c0 = P0[pv[a] * PN + pc];
-                const R li = R(0.5) * (Pm[pv[a] * PN + pc] + c0), hi = R(0.5) * (c0 + Pp[pv[a] * PN + pc]);
-                const R lj = R(0.5) * (P0[pv[a] * PN + pc - PK] + c0), hj = R(0.5) * (c0 + P0[pv[a] * PN + pc + PK]);
-                const R lk = R(0.5) * (P0[pv[a] * PN + pc - 1] + c0), hk = R(0.5) * (c0 + P0[pv[a] * PN + pc + 1]);
+                const R li = Pm[pv[a] * PN + pc] + c0, hi = c0 + Pp[pv[a] * PN + pc];
+                const R lj = P0[pv[a] * PN + pc - PK] + c0, hj = c0 + P0[pv[a] * PN + pc + PK];
+                const R lk = P0[pv[a] * PN + pc - 1] + c0, hk = c0 + P0[pv[a] * PN + pc + 1];
                 acc[3 * a] = ((hi * Hix - li * Six) + (hj * Hjx - lj * Sjx)) + (hk * Hkx - lk * Skx);
                 acc[3 * a + 1] = ((hi * Hiy - li * Siy) + (hj * Hjy - lj * Sjy)) + (hk * Hky - lk * Sky);
                 acc[3 * a + 2] = ((hi * Hiz - li * Siz) + (hj * Hjz - lj * Sjz)) + (hk * Hkz - lk * Skz);
             }
 #pragma unroll
-            for (int q = 0; q < 12; ++q) acc[q] *= hivol;
+            for (int q = 0; q < 12; ++q) acc[q] *= qivol;
             const R T = P0[PR_T * PN + pc];
             const R muh = R(0.5) * sutherland(T, P);              // half the molecular viscosity
             R muth = R(0);                                        // half the eddy viscosity
