@@ -41,13 +41,13 @@ N_CFG2 = (256, 128, 128)
 # DRAM bytes (read + write) per stage-kernel launch per interior cell, mean of the three RK
 # stages, from one ncu capture of the same kernel on a 128^3 case of this workload; scaled
 # by the cell count for the roofline's `traffic`
-TRAFFIC_PER_CELL = {"fp64": 325.0, "mixed": 229.0}
+TRAFFIC_PER_CELL = {"fp64": 327.0, "mixed": 229.0}
 # FP64 work per interior cell per stage-kernel launch (FP64 form, mean of the three RK
-# stages), from one ncu capture of the same kernel on a 128^3 case of this workload: DADD 285.6,
-# DMUL 366.5, DFMA 365.3 thread instructions, i.e. 1383 flop (an FMA counts two) in 1017
+# stages), from one ncu capture of the same kernel on a 128^3 case of this workload: DADD 277.8,
+# DMUL 329.5, DFMA 357.0 thread instructions, i.e. 1321 flop (an FMA counts two) in 964
 # FP64-pipe instructions
-FP64_FLOP_PER_CELL = 1383.0
-FP64_INST_PER_CELL = 1017.0
+FP64_FLOP_PER_CELL = 1321.0
+FP64_INST_PER_CELL = 964.0
 # nominal FP64 rate of a B200: 148 SMs x 64 FP64 lanes x 1.965 GHz (x 2 flop per FMA)
 FP64_PEAK_INST = 148 * 64 * 1.965e9
 FP64_PEAK_TFLOPS = 2 * FP64_PEAK_INST / 1e12
