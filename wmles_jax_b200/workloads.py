@@ -82,8 +82,16 @@ def loglaw_prim(gas, mesh, noise=0.1, seed=0):
 
     def prim(xc):
         y = xc[1]
-        ys, yi = np.unique(y, return_inverse=True)
-        u = (ut * spalding_uplus(np.clip(np.minimum(ys, 2.0 - ys), 0.0, None) * ut / nu))[yi.reshape(y.shape)]
+        # on a grid extruded in x and z (every channel grid here) y is one j-line repeated:
+        # the profile is evaluated on that line and broadcast, the same values as over all cells
+        line = y[:1, :, :1] if y.ndim == 3 else None
+        if line is not None and np.array_equal(y, np.broadcast_to(line, y.shape)):
+            ys, yi = np.unique(line, return_inverse=True)
+            u = np.broadcast_to((ut * spalding_uplus(np.clip(np.minimum(ys, 2.0 - ys), 0.0, None) * ut / nu))
+                                [yi.reshape(line.shape)], y.shape)
+        else:
+            ys, yi = np.unique(y, return_inverse=True)
+            u = (ut * spalding_uplus(np.clip(np.minimum(ys, 2.0 - ys), 0.0, None) * ut / nu))[yi.reshape(y.shape)]
         # noise of std `noise` U_b in the core, scaled by the mean-velocity shape towards the
         # walls: grid-scale noise at y+ ~ 1 gives an SGS viscosity far above the molecular
         # one, which the reference's CFL estimate (molecular viscosity only) does not cover
