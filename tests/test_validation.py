@@ -93,3 +93,26 @@ def test_ghost_program_indices_checked(lowered, prog, corrupt):
         p.op_code[0] = 77
     assert create() == E_INVALID, lib.wm_last_error()
     assert prog.encode() in lib.wm_last_error()
+
+
+def test_inflow_span_limit(W, monkeypatch):
+    """The synthetic inflow's row launch keeps a ghost row's three noise fields in 48 KB of
+    shared memory: a wider inflow block is refused at creation, not at the first fill."""
+    if torch.cuda.is_available():
+        pytest.skip("checks the path that stops before any device call")
+    from wmles_jax_b200 import _native as N
+    from wmles_jax_b200 import solver as S
+    if not os.path.exists(N.LIB_PATH):
+        from wmles_jax_b200.build import build
+        build()
+    monkeypatch.setattr(S, "require_gpu", lambda: torch.device("cpu"))
+    mesh, gas, kw, prim, t = C.golden_case(W, "ramp_small")
+    s = S.Solver.__new__(S.Solver)
+    s._prepare(mesh, gas, **kw)
+    lib = N.load()
+    h = ctypes.c_void_p()
+    assert s._desc.inflow
+    assert lib.wm_case_create(ctypes.byref(s._desc), ctypes.byref(h)) == E_CUDA
+    s._desc.blocks[s._desc.inflow.contents.block].n[2] = 2048
+    assert lib.wm_case_create(ctypes.byref(s._desc), ctypes.byref(h)) == E_UNSUPPORTED
+    assert b"inflow" in lib.wm_last_error()

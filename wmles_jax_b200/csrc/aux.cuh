@@ -114,8 +114,10 @@ struct InflowArgs {
 constexpr int IN_PARTS = 4;
 // kernel launches of one inflow fill (mode sums, then the rows)
 constexpr int IN_LAUNCHES = 2;
-// the rows' launch: one warp per velocity component of a ghost row
+// the rows' launch: one warp per velocity component of a ghost row; the row's three noise
+// fields sit in the launch's default shared memory (48 KB), which bounds the ghosted span
 constexpr int IN_ROW_NT = 96;
+constexpr int IN_ROW_MAX_NK = 48 * 1024 / (3 * 8);
 // extruded plane: ghost rows per CTA of the mode sums, threads per CTA, and the largest
 // dynamic shared memory of that launch (one component's cos / sin (kz z) table and the rows'
 // sincos of alpha)

@@ -290,6 +290,9 @@ int validate(const wm_case_desc* d) {
         if (I.block < 0 || I.block >= d->nblocks) return fail(WM_E_INVALID, "inflow block %d", I.block);
         if (I.n_modes < 1 || I.n_tab < 2 || !I.modes || !I.table) return fail(WM_E_INVALID, "bad inflow tables");
         if (!(I.L > 0)) return fail(WM_E_INVALID, "inflow length scale must be positive");
+        const int Nk = d->blocks[I.block].n[2] + 2 * d->blocks[I.block].ng;
+        if (Nk > IN_ROW_MAX_NK)
+            return fail(WM_E_UNSUPPORTED, "inflow block: %d cells along k with ghosts, above %d", Nk, IN_ROW_MAX_NK);
     }
     if (d->sponge.enabled && !(d->sponge.x_end_l > d->sponge.x_start_l && d->sponge.L > 0))
         return fail(WM_E_INVALID, "bad sponge extent");
