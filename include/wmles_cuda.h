@@ -99,7 +99,8 @@ typedef struct {
 } wm_ghost_program;
 
 typedef struct {
-    int block;                /* i-min face of this block */
+    int block;                /* i-min face of this block; at most 2048 cells along k with
+                                 ghosts (wider: WM_E_UNSUPPORTED at creation) */
     int n_modes, n_tab;
     const double* modes;      /* host, 3 x 4 x n_modes: kx, ky, kz, phase per component */
     const double* table;      /* host, n_tab x 7: y/L, U, V, uu, vv, ww, uv (by U_inf) */
