@@ -9,10 +9,13 @@
   1e-9 relative), on an isothermal and on an adiabatic wall;
 * wall-load integration (tests/test_multiblock.py:161-190): uniform stream in a unit box
   with wall-modelled j faces; force and moment per face against the closed forms;
+* multiblock consistency (tests/test_multiblock.py:88-98,216-219): two-block splits, and a
+  periodic chain of eight blocks, give the single block's RHS cell by cell;
+* sponge mean preservation (tests/test_smooth_ramp.py:74-96);
 * device placement (tests/test_multiblock.py:152-157): metrics and states on the device.
 
-The expected values are closed forms or an independent bisection written here, not the
-oracle.
+The expected values are closed forms, an independent bisection written here or the single
+block's own result, not the oracle.
 """
 import numpy as np
 import pytest
@@ -177,6 +180,47 @@ def test_multiblock_matches_single_block(W, kind, scheme, ybc, precision, tol):
     scale = np.max(np.abs(np.array(list(R[0].values()))))
     err = max(np.max(np.abs(R[0][c] - R[1][c])) for c in R[0]) / scale
     assert err < tol, err
+
+
+def _chain_case(W, pieces, n=(40, 10, 8)):
+    """The skewed periodic box cut into `pieces` blocks along i (uneven widths), each
+    connected to the next, the last to the first across the periodic shift; slip walls in y."""
+    cuts = np.linspace(0, n[0], pieces + 1).round().astype(int)
+    cuts[1:-1] += np.arange(1, pieces) % 2                  # uneven widths
+    assert np.all(np.diff(cuts) >= 3)
+    iy, iz = np.arange(n[1] + 1), np.arange(n[2] + 1)
+    blocks = [W.Block(f"b{p}", C.skew_nodes(np.arange(cuts[p], cuts[p + 1] + 1), iy, iz, n))
+              for p in range(pieces)]
+    mesh = W.Mesh(blocks)
+    for p in range(pieces - 1):
+        mesh.connect(blocks[p], "imax", blocks[p + 1], "imin")
+    mesh.connect(blocks[-1], "imax", blocks[0], "imin", shift=(C.LBOX[0], 0, 0))
+    for b in blocks:
+        mesh.connect(b, "kmin", b, "kmax", shift=(0, 0, -C.LBOX[2]))
+        b.set_bc("jmin", W.SlipWall())
+        b.set_bc("jmax", W.SlipWall())
+    mesh.finalize()
+    return mesh
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("mixed", 1e-5)])
+def test_many_blocks_match_single_block(W, precision, tol):
+    """Eight blocks of uneven widths in a periodic chain: the RHS and one step equal the
+    single block's (the gather keys by cell centre)."""
+    out = []
+    for pieces in (1, 8):
+        mesh = _chain_case(W, pieces)
+        s = _Solver(mesh, W.Gas(), W.KEP(4), sgs="wale", cfl=0.5, precision=precision)
+        Q = s.init_state(C.skew_prim)
+        Q1, dt = s.step(Q)
+        out.append((_gather(mesh, s.rhs(Q)), _gather(mesh, Q1), float(dt)))
+    for a, b in ((out[0][0], out[1][0]), (out[0][1], out[1][1])):
+        assert a.keys() == b.keys()
+        scale = np.max(np.abs(np.array(list(a.values()))))
+        err = max(np.max(np.abs(a[c] - b[c])) for c in a) / scale
+        assert err < tol, err
+    dt_tol = 1e-12 if precision == "fp64" else 1e-6      # the mixed form's CFL rates are FP32
+    assert abs(out[0][2] - out[1][2]) <= dt_tol * out[0][2]
 
 
 # ----------------------------------------------------------------------- sponge
