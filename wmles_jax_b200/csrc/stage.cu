@@ -48,16 +48,17 @@ constexpr int stage_min_ctas(size_t rsize, int nt) {
 // the first TJ x TK threads.  FP64 256-column tiles only, where one CTA per SM is resident.
 // The launch bound of the larger CTA holds the kernel at 168 (352 threads) or 128 registers
 // (448, 512 threads), with up to ~580 B of spills at 128, and it is still faster.  Measured
-// stage time per step, 8 x 32 tile (config 2 KEP / config 3 / config 4 Hybrid): 3.17 / 3.37 /
+// stage time per step, 8 x 32 tile (channel 256x128x128 KEP / smooth ramp 384x96x64 / NACA
+// C-grid 576x64x40, Hybrid): 3.17 / 3.37 /
 // 3.72 ms at 256 threads (254 registers), 2.81 / 3.08 / 3.74 at 352, 2.65 / 2.81 / 3.20 at
 // 448, 2.67 / 2.78 / 3.03 at 512; 16 x 16 tile: KEP 2.93 at 448 (3.03 at 352), Hybrid
 // 3.12 / 2.61 at 352 (3.17 / 2.77 at 384, 3.52 / 2.85 at 512).  Since the FP64 form's two
 // phases per plane (below), KEP runs 512 threads as well: 16 warps are charged the registers
-// of 14 (groups of four), and the conversion gets five warps (config 2 stage per step 2.586
+// of 14 (groups of four), and the conversion gets five warps (channel stage per step 2.586
 // against 2.598 ms at 448).  The float form's two-CTA
 // tiles (issue-bound rather than latency-bound) gain nothing measurable and keep their
 // columns' threads; its one-CTA 16 x 32 tile runs 640 threads at 96 registers (mixed stage
-// time per step, configs 2 / 3 / 4: 1.52 / 1.23 / 1.14 ms, against 1.65 / 1.36 / 1.23 at
+// time per step, channel / ramp / C-grid: 1.52 / 1.23 / 1.14 ms, against 1.65 / 1.36 / 1.23 at
 // 512 threads and 1.58 / 1.31 / 1.21 for the best two-CTA tile).
 constexpr int STAGE_MAX_WARPS = 32;          // two reduction sums per warp in the scratch
 constexpr int stage_extra_warps(size_t rsize, int scheme, int tj, int tk) {
@@ -82,15 +83,15 @@ struct StageLayout {
     // FP64, one CTA per SM: a fifth primitive slot (the shared memory is there), so plane
     // i+2 is converted while the gradient records of plane i are computed, by the warps that
     // have no record to compute, and a plane takes two barriers instead of three.  FP64 stage
-    // time per step, channel 256x128x128 / smooth ramp 384x96x64 / NACA C-grid (configs 2 / 3 /
-    // 4): 2.62 / 2.63 / 2.91 ms against 2.70 / 2.75 / 2.93 with three phases.  The float
+    // time per step, channel 256x128x128 / smooth ramp 384x96x64 / NACA C-grid 576x64x40:
+    // 2.62 / 2.63 / 2.91 ms against 2.70 / 2.75 / 2.93 with three phases.  The float
     // form's one-CTA 16 x 32 tile has a record for nearly every thread (612 records, 640
     // threads) and gains nothing (ramp / C-grid 1.17 / 1.09 ms against 1.17 / 1.08): it keeps
     // three phases.
     static constexpr bool FUSE = MIN_CTAS == 1 && sizeof(R) == 8;
     static constexpr int NSLOT = FUSE ? 5 : 4;
     // KEP in the two-phase form: the RK epilogue deferred to the next gradient phase (below).
-    // Config 2 stage per step 2.546 ms against 2.583; the Hybrid kernels, whose gradient phase
+    // Channel 256x128x128 stage per step 2.546 ms against 2.583; the Hybrid kernels, whose gradient phase
     // is the longer one, lose with it (ramp +0.5 %, C-grid +6.4 %) and keep it in the face phase.
     static constexpr bool DEFER = FUSE && SCHEME == WM_SCHEME_KEP;
     static constexpr size_t qs_off = 0;                                        // double [5][PN]
